@@ -1,0 +1,1566 @@
+// fi_api.cu -- the C ABI (include/fastiso_b200.h): handle lifecycle, FP64 set-up,
+// the fused FP32 step loop as a CUDA graph (conditional WHILE over BS3 steps,
+// conditional IF per sparse update), and the plain FP64 form with a host-side
+// step controller.  Integrator semantics: OrdinaryDiffEq BS3 as driven by
+// run!/init_integrator/step! (src/simulation.jl:236-322).
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/fastiso_b200.h"
+#include "fi_device.cuh"
+#include "fi_kernels.h"
+#include "fi_plain.h"
+
+using namespace fi;
+
+namespace {
+
+constexpr int NT = 256;
+
+inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+struct Plan {
+    int L;
+    int npass;
+    int radix[FFT_MAX_PASSES];
+    float2* tw32;
+    double2* tw64;
+};
+
+struct PlainBufs {
+    double *u[2], *k14[2], *k2, *k3, *tmp, *uin, *fscratch;
+    double *now_u, *ue, *dz, *H, *H_af, *z_b, *z_ss, *s_i, *s_l, *s_m, *s_load, *s_full, *dudt;
+    double *rhs, *bxx, *byy, *bx, *bxy, *Mxx, *Myy, *Mxy, *buf, *cropped, *off, *partial;
+    double2 *fftrhs, *P;
+    double *D, *eta, *mask, *u_ref, *ue_ref, *z_b_ref, *z_ss_ref, *H_af_ref, *H_tab;
+    double2 *Ge_hat, *Gg_hat;
+};
+
+}  // namespace
+
+struct fi_handle {
+    fi_config cfg;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    int nx, ny, NH, sp, Mx, My, MH, msp, mx, my, i1, j1;
+    double dx, dy;
+    std::vector<void*> allocs;
+    // FFT plans
+    std::map<int, int> plan_of_len;
+    std::vector<Plan> plans;
+    FftPlan* d_plans = nullptr;
+    int plan_x, plan_y, plan_Mx, plan_My;
+    // host-side inputs
+    std::vector<double> D, eta, R, mask, u_ref, ue_ref, dz_ss_ref, z_b_ref, u_init;
+    bool R_given = false, u_set = false;
+    std::vector<double> ice_t, ice_H;
+    std::vector<double> rm, GE;
+    std::vector<double> ch_ratio, ch_thick;
+    // FP64 set-up products
+    double *d_pd = nullptr, *d_R = nullptr, *d_spinv = nullptr, *d_Ge = nullptr, *d_Gg = nullptr;
+    double2 *d_P64 = nullptr;
+    std::vector<double> H_ice_ref, H_af_ref, z_ss_ref;
+    // fused form
+    Member mem{};
+    Member* d_mem = nullptr;
+    Ctl* d_ctl = nullptr;
+    Task *t_rows = nullptr, *t_cols = nullptr, *t_crow = nullptr, *t_ccol = nullptr, *t_crowi = nullptr;
+    int n_rows, n_cols, n_crow, n_ccol, n_crowi;
+    int h_rows = 2, B_cols = 2, h_conv = 2, B_conv = 1;
+    double* d_uin = nullptr;
+    float* d_vscr = nullptr;
+    double* d_cscr = nullptr;
+    double* d_red = nullptr;
+    int red_blocks = 0;
+    double* d_tout = nullptr;
+    cudaGraphExec_t seg_exec = nullptr;
+    cudaGraph_t seg_graph = nullptr;
+    bool graph_ok = true;
+    // plain form
+    PlainBufs p{};
+    // integrator (host mirror for the plain form; snapshot for the fused form)
+    Ctl ctl{};
+    std::vector<double> tstops, tout;
+    bool initialized = false, integ_started = false;
+    int last_call = 0;  // 0: step loop, 1: fi_rhs
+    bool fsal_pending = false;  // FSAL re-evaluation owed by the last output callback
+    double last_rhs_t = 0.0;
+    long long nf_plain = 0;
+};
+
+static int set_err(fi_handle* h, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    h->err = buf;
+    return code;
+}
+
+#define CK(x)                                                                                         \
+    do {                                                                                              \
+        cudaError_t e__ = (x);                                                                        \
+        if (e__ != cudaSuccess)                                                                       \
+            return set_err(h, FI_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #x, cudaGetErrorString(e__)); \
+    } while (0)
+
+#define CKL()                                                                                         \
+    do {                                                                                              \
+        cudaError_t e__ = cudaGetLastError();                                                         \
+        if (e__ != cudaSuccess)                                                                       \
+            return set_err(h, FI_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__, cudaGetErrorString(e__)); \
+    } while (0)
+
+#define RET(x)                 \
+    do {                       \
+        int r__ = (x);         \
+        if (r__) return r__;   \
+    } while (0)
+
+template <typename T>
+static int dalloc(fi_handle* h, T** p, size_t n) {
+    void* q = nullptr;
+    CK(cudaMalloc(&q, (n ? n : 1) * sizeof(T)));
+    CK(cudaMemsetAsync(q, 0, (n ? n : 1) * sizeof(T), h->stream));
+    h->allocs.push_back(q);
+    *p = (T*)q;
+    return FI_OK;
+}
+
+static int get_plan(fi_handle* h, int L, int* out) {
+    auto it = h->plan_of_len.find(L);
+    if (it != h->plan_of_len.end()) { *out = it->second; return FI_OK; }
+    if (L < 1 || L > FFT_MAX_LEN) return set_err(h, FI_ERR_ARG, "transform length %d outside [1, %d]", L, FFT_MAX_LEN);
+    Plan p{};
+    p.L = L;
+    int m = L, np = 0;
+    while (m % 8 == 0) { p.radix[np++] = 8; m /= 8; }
+    while (m % 4 == 0) { p.radix[np++] = 4; m /= 4; }
+    while (m % 2 == 0) { p.radix[np++] = 2; m /= 2; }
+    const int small[3] = {7, 5, 3};
+    for (int q : small) while (m % q == 0) { p.radix[np++] = q; m /= q; }
+    for (int f = 11; f * f <= m; f += 2) while (m % f == 0) { p.radix[np++] = f; m /= f; }
+    if (m > 1) p.radix[np++] = m;
+    p.npass = np;
+    std::vector<double2> t64(L);
+    std::vector<float2> t32(L);
+    for (int k = 0; k < L; k++) {
+        const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)L;
+        t64[k] = make_double2((double)cosl(a), (double)sinl(a));
+        t32[k] = make_float2((float)t64[k].x, (float)t64[k].y);
+    }
+    RET(dalloc(h, &p.tw64, L));
+    RET(dalloc(h, &p.tw32, L));
+    CK(cudaMemcpyAsync(p.tw64, t64.data(), L * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(p.tw32, t32.data(), L * sizeof(float2), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *out = (int)h->plans.size();
+    h->plan_of_len[L] = *out;
+    h->plans.push_back(p);
+    return FI_OK;
+}
+
+static int upload_plans(fi_handle* h) {
+    std::vector<FftPlan> v(h->plans.size());
+    for (size_t i = 0; i < v.size(); i++) {
+        v[i].L = h->plans[i].L;
+        v[i].npass = h->plans[i].npass;
+        memcpy(v[i].radix, h->plans[i].radix, sizeof(v[i].radix));
+        v[i].tw32 = h->plans[i].tw32;
+        v[i].tw64 = h->plans[i].tw64;
+    }
+    RET(dalloc(h, &h->d_plans, v.size()));
+    CK(cudaMemcpyAsync(h->d_plans, v.data(), v.size() * sizeof(FftPlan), cudaMemcpyHostToDevice, h->stream));
+    return FI_OK;
+}
+
+static int nextfastfft(int n) {
+    for (int m = std::max(n, 1);; m++) {
+        int r = m;
+        for (int p : {2, 3, 5, 7}) while (r % p == 0) r /= p;
+        if (r == 1) return m;
+    }
+}
+
+static inline size_t N2(const fi_handle* h) { return (size_t)h->nx * h->ny; }
+
+extern "C" {
+
+void fi_config_default(fi_config* c, int32_t nx, int32_t ny, double Wx, double Wy) {
+    memset(c, 0, sizeof(*c));
+    c->nx = nx; c->ny = ny; c->Wx = Wx; c->Wy = Wy;
+    c->mE = 5.972e24;
+    c->r_pole = 6357e3;
+    c->g = 9.8;
+    c->seconds_per_year = 60.0 * 60.0 * 24 * 365.25;
+    c->rho_ice = 0.910e3;
+    c->rho_water = 1e3;
+    c->rho_seawater = 1.023e3;
+    c->rho_litho = 3.2e3;
+    c->rho_uppermantle = 3.4e3;
+    c->litho_poissonratio = 0.28;
+    c->lithosphere = FI_LITHO_LATERALLY_VARIABLE;
+    c->lithosphere_column = FI_COLUMN_INCOMPRESSIBLE;
+    c->sea_surface = FI_SEA_SURFACE_LATERALLY_CONSTANT;
+    c->ice_mode = FI_ICE_TIME_INTERPOLATED;
+    c->t0 = 0.0;
+    c->t1 = 1.0;
+    c->reltol = (double)1e-5f;
+    c->abstol = 1e-6;
+    c->dt_sparse_diagnostics = 10.0;
+    c->max_steps = 1000000;
+    c->form = FI_FORM_FP32;
+}
+
+const char* fi_status_string(int32_t s) {
+    switch (s) {
+        case FI_OK: return "ok";
+        case FI_ERR_ARG: return "invalid argument";
+        case FI_ERR_CUDA: return "CUDA error";
+        case FI_ERR_NONFINITE: return "non-finite value in the state or error norm";
+        case FI_ERR_DT_UNDERFLOW: return "dt below dtmin";
+        case FI_ERR_FORCING_RANGE: return "TimeInterpolation2D out of range.";
+        case FI_ERR_TIMEOUT: return "device wait timed out";
+        case FI_ERR_STATE: return "call out of lifecycle order";
+        case FI_ERR_UNSUPPORTED: return "option outside the LV-ELVA path";
+        case FI_ERR_MAXITERS: return "maximum number of steps reached";
+        default: return "unknown";
+    }
+}
+
+const char* fi_last_error(const fi_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+static int create_buffers(fi_handle* h);
+
+int fi_create(const fi_config* cfg, fi_handle** out) {
+    if (!cfg || !out) return FI_ERR_ARG;
+    *out = nullptr;
+    if (cfg->nx < 4 || cfg->ny < 4 || cfg->nx > 2048 || cfg->ny > 2048) return FI_ERR_ARG;
+    if (!(cfg->Wx > 0) || !(cfg->Wy > 0) || !(cfg->t1 >= cfg->t0)) return FI_ERR_ARG;
+    if (cfg->form != FI_FORM_FP32 && cfg->form != FI_FORM_FP64) return FI_ERR_ARG;
+    fi_handle* h = new fi_handle();
+    h->cfg = *cfg;
+    h->nx = cfg->nx; h->ny = cfg->ny;
+    h->mx = h->nx / 2; h->my = h->ny / 2;
+    h->NH = h->nx / 2 + 1;
+    h->sp = round_up(h->NH, 16);
+    h->Mx = nextfastfft(2 * h->nx - 1);
+    h->My = nextfastfft(2 * h->ny - 1);
+    h->MH = h->Mx / 2 + 1;
+    h->msp = round_up(h->MH, 16);
+    h->i1 = (h->nx % 2 == 0) ? h->mx - 1 : h->mx;  // samesize_conv_indices, 0-based
+    h->j1 = (h->ny % 2 == 0) ? h->my - 1 : h->my;
+    h->dx = 2 * cfg->Wx / h->nx;
+    h->dy = 2 * cfg->Wy / h->ny;
+    const size_t n = N2(h);
+    h->D.assign(n, 0.0);
+    h->eta.assign(n, 0.0);
+    h->R.assign(n, 1.0);
+    h->mask.assign(n, 1.0);
+    h->u_ref.assign(n, 0.0);
+    h->ue_ref.assign(n, 0.0);
+    h->dz_ss_ref.assign(n, 0.0);
+    h->z_b_ref.assign(n, 1e6);
+    h->u_init.assign(n, 0.0);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return FI_ERR_CUDA;
+    }
+    int rc = create_buffers(h);
+    if (rc) {
+        fprintf(stderr, "fi_create: %s\n", h->err.c_str());
+        fi_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return FI_OK;
+}
+
+void fi_destroy(fi_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->seg_exec) cudaGraphExecDestroy(h->seg_exec);
+    if (h->seg_graph) cudaGraphDestroy(h->seg_graph);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// buffers
+// ---------------------------------------------------------------------------
+static int create_buffers(fi_handle* h) {
+    const size_t n = N2(h);
+    RET(get_plan(h, h->nx, &h->plan_x));
+    RET(get_plan(h, h->ny, &h->plan_y));
+    RET(get_plan(h, h->Mx, &h->plan_Mx));
+    RET(get_plan(h, h->My, &h->plan_My));
+    RET(upload_plans(h));
+    RET(dalloc(h, &h->d_pd, n));
+    RET(dalloc(h, &h->d_R, n));
+    RET(dalloc(h, &h->d_spinv, n));
+    RET(dalloc(h, &h->d_Ge, n));
+    RET(dalloc(h, &h->d_Gg, n));
+    RET(dalloc(h, &h->d_P64, (size_t)h->Mx * h->My));
+    h->red_blocks = std::min(1024, cdiv((long long)n, NT));
+    RET(dalloc(h, &h->d_red, 2 * (size_t)h->red_blocks));
+    RET(dalloc(h, &h->d_tout, MAX_TSTOPS));
+    if (h->cfg.form == FI_FORM_FP32) {
+        Member& m = h->mem;
+        m.nx = h->nx; m.ny = h->ny; m.NH = h->NH; m.sp = h->sp;
+        m.Mx = h->Mx; m.My = h->My; m.MH = h->MH; m.msp = h->msp;
+        m.i1 = h->i1; m.j1 = h->j1;
+        m.plan_x = h->plan_x; m.plan_y = h->plan_y; m.plan_Mx = h->plan_Mx; m.plan_My = h->plan_My;
+        for (int b = 0; b < 2; b++) {
+            RET(dalloc(h, &m.u[b], n));
+            RET(dalloc(h, &m.k14[b], n));
+            RET(dalloc(h, &m.ue[b], n));
+        }
+        RET(dalloc(h, &m.k2, n));
+        RET(dalloc(h, &m.k3, n));
+        float *D, *vf, *mult, *mask, *hafref, *sigref, *zbss, *ueref, *Hext;
+        RET(dalloc(h, &D, n)); m.D = D;
+        RET(dalloc(h, &vf, n)); m.visc_fac = vf;
+        RET(dalloc(h, &mult, (size_t)h->NH * h->ny)); m.mult = mult;
+        RET(dalloc(h, &mask, n)); m.mask = mask;
+        RET(dalloc(h, &hafref, n)); m.H_af_ref = hafref;
+        RET(dalloc(h, &sigref, n)); m.sigma_ref = sigref;
+        RET(dalloc(h, &zbss, n)); m.zbss_ref = zbss;
+        RET(dalloc(h, &ueref, n)); m.ue_ref = ueref;
+        RET(dalloc(h, &Hext, n)); m.H_ext = Hext;
+        RET(dalloc(h, &m.dz, n));
+        RET(dalloc(h, &m.sig_load, n));
+        RET(dalloc(h, &m.sig_geo, n));
+        RET(dalloc(h, &m.S, (size_t)h->ny * h->sp));
+        RET(dalloc(h, &m.SA, (size_t)h->ny * h->msp));
+        RET(dalloc(h, &m.SB, (size_t)h->ny * h->msp));
+        RET(dalloc(h, &m.TA, (size_t)(h->ny + 2) * h->msp));
+        RET(dalloc(h, &m.TB, (size_t)(h->ny + 2) * h->msp));
+        float2 *GA, *GB;
+        RET(dalloc(h, &GA, (size_t)h->MH * h->My)); m.GA = GA;
+        RET(dalloc(h, &GB, (size_t)h->MH * h->My)); m.GB = GB;
+        RET(dalloc(h, &m.partial, (size_t)h->ny + 16));
+        RET(dalloc(h, &h->d_ctl, 1));
+        m.ctl = h->d_ctl;
+        m.tout = h->d_tout;
+        RET(dalloc(h, &h->d_uin, n));
+        RET(dalloc(h, &h->d_vscr, n));
+        RET(dalloc(h, &h->d_cscr, 8));
+        RET(dalloc(h, &h->d_mem, 1));
+        // tunables
+        h->h_rows = 2;
+        h->B_cols = h->ny >= 768 ? 1 : 2;
+        h->h_conv = h->Mx >= 1024 ? 1 : 2;
+        h->B_conv = 1;
+        h->n_rows = cdiv(h->ny, h->h_rows);
+        h->n_cols = cdiv(h->NH, h->B_cols);
+        h->n_crow = cdiv(h->ny, h->h_conv);
+        h->n_ccol = cdiv(h->MH, h->B_conv);
+        h->n_crowi = cdiv(h->ny + 2, h->h_conv);
+        auto mk = [&](Task** dst, int count) -> int {
+            std::vector<Task> t(count);
+            for (int i = 0; i < count; i++) t[i] = Task{0, i};
+            RET(dalloc(h, dst, count));
+            CK(cudaMemcpyAsync(*dst, t.data(), count * sizeof(Task), cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            return FI_OK;
+        };
+        RET(mk(&h->t_rows, h->n_rows));
+        RET(mk(&h->t_cols, h->n_cols));
+        RET(mk(&h->t_crow, h->n_crow));
+        RET(mk(&h->t_ccol, h->n_ccol));
+        RET(mk(&h->t_crowi, h->n_crowi));
+        const size_t smax = 227 * 1024;
+        const size_t s1 = rows_fwd_smem(h->nx, h->h_rows), s2 = cols_smem(h->ny, h->B_cols),
+                     s3 = rows_inv_smem(h->nx, h->h_rows), s4 = conv_rows_smem(h->Mx, h->h_conv),
+                     s5 = conv_cols_smem(h->My, h->B_conv);
+        if (s1 > smax || s2 > smax || s3 > smax || s4 > smax || s5 > smax)
+            return set_err(h, FI_ERR_ARG, "shared memory need exceeds 227 KB");
+        CK(cudaFuncSetAttribute(k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+        CK(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
+        CK(cudaFuncSetAttribute(k_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3));
+        CK(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4));
+        CK(cudaFuncSetAttribute(k_conv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s5));
+        CK(cudaFuncSetAttribute(k_conv_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4));
+    } else {
+        PlainBufs& p = h->p;
+        const size_t M = (size_t)h->Mx * h->My;
+        double** bufs[] = {&p.u[0], &p.u[1], &p.k14[0], &p.k14[1], &p.k2, &p.k3, &p.tmp, &p.uin, &p.fscratch,
+                           &p.now_u, &p.ue, &p.dz, &p.H, &p.H_af, &p.z_b, &p.z_ss, &p.s_i, &p.s_l, &p.s_m,
+                           &p.s_load, &p.s_full, &p.dudt, &p.rhs, &p.bxx, &p.byy, &p.bx, &p.bxy, &p.Mxx,
+                           &p.Myy, &p.Mxy, &p.buf, &p.D, &p.eta, &p.mask, &p.u_ref, &p.ue_ref, &p.z_b_ref,
+                           &p.z_ss_ref, &p.H_af_ref};
+        for (double** b : bufs) RET(dalloc(h, b, n));
+        RET(dalloc(h, &p.cropped, (size_t)(2 * h->nx - 1) * (2 * h->ny - 1)));
+        RET(dalloc(h, &p.off, 4));
+        RET(dalloc(h, &p.partial, 2 * (size_t)h->red_blocks));
+        RET(dalloc(h, &p.fftrhs, n));
+        RET(dalloc(h, &p.P, M));
+        RET(dalloc(h, &p.Ge_hat, M));
+        RET(dalloc(h, &p.Gg_hat, M));
+        const size_t s1 = fft64_rows_smem(std::max(h->nx, h->Mx), 1), s2 = fft64_cols_smem(std::max(h->ny, h->My), 1);
+        CK(cudaFuncSetAttribute(k_fft64_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+        CK(cudaFuncSetAttribute(k_fft64_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
+    }
+    if (h->cfg.form == FI_FORM_FP32) {
+        // FP64 transforms of the set-up are needed by both forms
+        const size_t s1 = fft64_rows_smem(h->Mx, 1), s2 = fft64_cols_smem(h->My, 1);
+        CK(cudaFuncSetAttribute(k_fft64_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+        CK(cudaFuncSetAttribute(k_fft64_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return FI_OK;
+}
+
+// FP64 2D transform of an nx-by-ny complex plane with row pitch nx (1 line per block)
+static int fft2_64(fi_handle* h, double2* a, int nx, int ny, int inverse) {
+    int px, py;
+    RET(get_plan(h, nx, &px));
+    RET(get_plan(h, ny, &py));
+    const double scale = inverse ? 1.0 / ((double)nx * ny) : 1.0;
+    if (!inverse) {
+        k_fft64_rows<<<ny, NT, fft64_rows_smem(nx, 1), h->stream>>>(a, nx, ny, nx, h->d_plans, px, 0, 1);
+        CKL();
+        k_fft64_cols<<<nx, NT, fft64_cols_smem(ny, 1), h->stream>>>(a, nx, ny, nx, h->d_plans, py, 0, 1, 1.0);
+        CKL();
+    } else {
+        k_fft64_cols<<<nx, NT, fft64_cols_smem(ny, 1), h->stream>>>(a, nx, ny, nx, h->d_plans, py, 1, 1, scale);
+        CKL();
+        k_fft64_rows<<<ny, NT, fft64_rows_smem(nx, 1), h->stream>>>(a, nx, ny, nx, h->d_plans, px, 1, 1);
+        CKL();
+    }
+    return FI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// field access
+// ---------------------------------------------------------------------------
+template <typename T>
+static int upload(fi_handle* h, T* dst, const std::vector<double>& src) {
+    std::vector<T> tmp(src.begin(), src.end());
+    CK(cudaMemcpyAsync(dst, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return FI_OK;
+}
+
+template <typename T>
+static int download(fi_handle* h, std::vector<double>& dst, const T* src, size_t n) {
+    std::vector<T> tmp(n);
+    CK(cudaMemcpyAsync(tmp.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    dst.assign(tmp.begin(), tmp.end());
+    return FI_OK;
+}
+
+static int read_ctl(fi_handle* h) {
+    if (h->cfg.form != FI_FORM_FP32) return FI_OK;
+    CK(cudaMemcpyAsync(&h->ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return FI_OK;
+}
+
+static int write_ctl(fi_handle* h) {
+    if (h->cfg.form != FI_FORM_FP32) return FI_OK;
+    CK(cudaMemcpyAsync(h->d_ctl, &h->ctl, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return FI_OK;
+}
+
+static double corner_mean(const double* c) { return 0.25 * (c[0] + c[1] + c[2] + c[3]); }
+
+static void interp_ice_host(const fi_handle* h, double t, std::vector<double>& H, int* status) {
+    const size_t n = N2(h);
+    H.assign(n, 0.0);
+    *status = FI_OK;
+    if (h->cfg.ice_mode != FI_ICE_TIME_INTERPOLATED || h->ice_t.empty()) return;
+    const std::vector<double>& tt = h->ice_t;
+    const int K = (int)tt.size();
+    int i;
+    if (t < tt[0] || t > tt[K - 1]) {
+        if (!h->cfg.ice_flat_bc) { *status = FI_ERR_FORCING_RANGE; return; }
+        i = t < tt[0] ? 0 : K - 1;
+        std::copy(h->ice_H.begin() + (size_t)i * n, h->ice_H.begin() + (size_t)(i + 1) * n, H.begin());
+        return;
+    }
+    i = (int)(std::lower_bound(tt.begin(), tt.end(), t) - tt.begin());
+    if (tt[i] == t) {
+        std::copy(h->ice_H.begin() + (size_t)i * n, h->ice_H.begin() + (size_t)(i + 1) * n, H.begin());
+        return;
+    }
+    i -= 1;
+    const double* a = &h->ice_H[(size_t)i * n];
+    const double* b = &h->ice_H[(size_t)(i + 1) * n];
+    const double dti = tt[i + 1] - tt[i], ts = t - tt[i];
+    for (size_t k = 0; k < n; k++) H[k] = a[k] + (b[k] - a[k]) / dti * ts;
+}
+
+static double haf_host(double rho_sw_ice, double H, double zb, double zss) {
+    double m = zb - zss;
+    if (m > 0) m = 0;
+    const double v = H + m * rho_sw_ice;
+    return v > 0 ? v : 0.0;
+}
+
+extern "C" int fi_set_field(fi_handle* h, int32_t field, const double* host, size_t n) {
+    if (!h || !host) return FI_ERR_ARG;
+    if (n != N2(h)) return set_err(h, FI_ERR_ARG, "field size %zu != nx*ny", n);
+    std::vector<double> v(host, host + n);
+    switch (field) {
+        case FI_FIELD_LITHO_RIGIDITY: h->D = v; return FI_OK;
+        case FI_FIELD_EFFECTIVE_VISCOSITY: h->eta = v; return FI_OK;
+        case FI_FIELD_PSEUDODIFF_SCALING: h->R = v; h->R_given = true; return FI_OK;
+        case FI_FIELD_MASKACTIVE: h->mask = v; return FI_OK;
+        case FI_FIELD_U_REF: h->u_ref = v; return FI_OK;
+        case FI_FIELD_UE_REF: h->ue_ref = v; return FI_OK;
+        case FI_FIELD_DZ_SS_REF: h->dz_ss_ref = v; return FI_OK;
+        case FI_FIELD_Z_B_REF: h->z_b_ref = v; return FI_OK;
+        case FI_FIELD_U:
+            if (!h->initialized) { h->u_init = v; h->u_set = true; return FI_OK; }
+            if (h->cfg.form == FI_FORM_FP32) {
+                RET(read_ctl(h));
+                CK(cudaMemcpyAsync(h->mem.u[h->ctl.ibuf], host, n * 8, cudaMemcpyHostToDevice, h->stream));
+            } else {
+                CK(cudaMemcpyAsync(h->p.u[h->ctl.ibuf], host, n * 8, cudaMemcpyHostToDevice, h->stream));
+            }
+            CK(cudaStreamSynchronize(h->stream));
+            return FI_OK;
+        case FI_FIELD_H_ICE:
+            if (h->cfg.ice_mode != FI_ICE_EXTERNAL)
+                return set_err(h, FI_ERR_ARG, "H_ice is set externally only with FI_ICE_EXTERNAL");
+            if (h->cfg.form == FI_FORM_FP32) return upload(h, h->mem.H_ext, v);
+            return upload(h, h->p.H, v);
+        default: return set_err(h, FI_ERR_ARG, "field %d is not settable", field);
+    }
+}
+
+extern "C" int fi_set_ice_history(fi_handle* h, int32_t K, const double* t, const double* H) {
+    if (!h || K < 1 || !t || !H) return FI_ERR_ARG;
+    for (int k = 1; k < K; k++)
+        if (!(t[k] > t[k - 1])) return set_err(h, FI_ERR_ARG, "ice times must increase");
+    h->ice_t.assign(t, t + K);
+    h->ice_H.assign(H, H + (size_t)K * N2(h));
+    return FI_OK;
+}
+
+extern "C" int fi_set_elastic_table(fi_handle* h, int32_t n, const double* rm, const double* GE) {
+    if (!h || n < 2 || !rm || !GE) return FI_ERR_ARG;
+    h->rm.assign(rm, rm + n);
+    h->GE.assign(GE, GE + n);
+    return FI_OK;
+}
+
+extern "C" int fi_set_channel_scaling(fi_handle* h, int32_t n, const double* ratio, const double* thick) {
+    if (!h || n < 0 || (n > 0 && (!ratio || !thick))) return FI_ERR_ARG;
+    h->ch_ratio.assign(ratio, ratio + n);
+    h->ch_thick.assign(thick, thick + n);
+    return FI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// set-up (Simulation constructor tail)
+// ---------------------------------------------------------------------------
+static int build_kernel_spectrum(fi_handle* h, const double* G, float2* half32, double2* full64) {
+    const size_t M = (size_t)h->Mx * h->My;
+    k_pad_real<<<cdiv(M, NT), NT, 0, h->stream>>>(G, h->nx, h->ny, h->d_P64, h->Mx, h->My);
+    CKL();
+    RET(fft2_64(h, h->d_P64, h->Mx, h->My, 0));
+    if (half32) {
+        k_half_spectrum32<<<cdiv((size_t)h->MH * h->My, NT), NT, 0, h->stream>>>(
+            h->d_P64, h->Mx, h->My, h->MH, 1.0 / ((double)h->Mx * h->My), half32);
+        CKL();
+    }
+    if (full64) CK(cudaMemcpyAsync(full64, h->d_P64, M * sizeof(double2), cudaMemcpyDeviceToDevice, h->stream));
+    return FI_OK;
+}
+
+static int rhs_fused(fi_handle* h, int stage, const double* uin, float* vout, double* cout);
+static int rhs_plain(fi_handle* h, double t, double* u, double* dudt);
+
+extern "C" int fi_init(fi_handle* h) {
+    if (!h) return FI_ERR_ARG;
+    if (h->initialized) return set_err(h, FI_ERR_STATE, "fi_init called twice");
+    const fi_config& c = h->cfg;
+    const size_t n = N2(h);
+    for (size_t k = 0; k < n; k++)
+        if (!(h->eta[k] > 0) || !(h->D[k] >= 0))
+            return set_err(h, FI_ERR_ARG, "litho_rigidity / effective_viscosity not set (or non-positive)");
+    if (c.ice_mode == FI_ICE_TIME_INTERPOLATED && h->ice_t.empty())
+        return set_err(h, FI_ERR_STATE, "ice history not set");
+    const bool elastic = c.lithosphere != FI_LITHO_RIGID, geoid = c.sea_surface == FI_SEA_SURFACE_LATERALLY_VARIABLE;
+    if (elastic && h->rm.size() < 2) return set_err(h, FI_ERR_STATE, "elastic Green table not set");
+    // spectral factors and Green's functions, FP64 on the device
+    double *d_ratio = nullptr, *d_thick = nullptr, *d_Rg = nullptr;
+    const int nch = (int)h->ch_ratio.size();
+    RET(dalloc(h, &d_ratio, std::max(nch, 1)));
+    RET(dalloc(h, &d_thick, std::max(nch, 1)));
+    if (nch) {
+        RET(upload(h, d_ratio, h->ch_ratio));
+        RET(upload(h, d_thick, h->ch_thick));
+    }
+    if (h->R_given) {
+        RET(dalloc(h, &d_Rg, n));
+        RET(upload(h, d_Rg, h->R));
+    }
+    float* mult = (c.form == FI_FORM_FP32) ? (float*)h->mem.mult : nullptr;
+    float* mult_tmp = nullptr;
+    if (!mult) RET(dalloc(h, &mult_tmp, (size_t)h->NH * h->ny));
+    k_spectral_factors<<<cdiv(n, NT), NT, 0, h->stream>>>(h->nx, h->ny, c.Wx, c.Wy, nch, d_ratio, d_thick, d_Rg,
+                                                           c.seconds_per_year, h->d_pd, h->d_R, h->d_spinv,
+                                                           mult ? mult : mult_tmp, h->NH);
+    CKL();
+    double *d_rm = nullptr, *d_GE = nullptr;
+    if (elastic) {
+        RET(dalloc(h, &d_rm, h->rm.size()));
+        RET(dalloc(h, &d_GE, h->GE.size()));
+        RET(upload(h, d_rm, h->rm));
+        RET(upload(h, d_GE, h->GE));
+        k_elastic_green<<<cdiv(n, NT), NT, 0, h->stream>>>(h->d_Ge, h->nx, h->ny, h->mx, h->my, h->dx, h->dy, d_rm,
+                                                            d_GE, (int)h->rm.size());
+        CKL();
+    }
+    k_geoid_green<<<cdiv(n, NT), NT, 0, h->stream>>>(h->d_Gg, h->nx, h->ny, c.Wx, c.Wy, h->dx, h->dy, c.r_pole, c.mE);
+    CKL();
+    // reference state (src/simulation.jl:132-151) in FP64 on the host
+    int st;
+    interp_ice_host(h, c.t0, h->H_ice_ref, &st);
+    if (st) return set_err(h, st, "TimeInterpolation2D out of range.");
+    h->z_ss_ref.resize(n);
+    h->H_af_ref.resize(n);
+    const double rsi = c.rho_seawater / c.rho_ice;
+    for (size_t k = 0; k < n; k++) {
+        h->z_ss_ref[k] = c.z_bsl + h->dz_ss_ref[k];
+        h->H_af_ref[k] = haf_host(rsi, h->H_ice_ref[k], h->z_b_ref[k], h->z_ss_ref[k]);
+    }
+    std::vector<double> u0 = h->u_set ? h->u_init : h->u_ref;
+    Ctl& ct = h->ctl;
+    memset(&ct, 0, sizeof(Ctl));
+    ct.t = c.t0; ct.t0 = c.t0; ct.t1 = c.t1;
+    ct.dtmax = c.t1 - c.t0;
+    ct.dtmin = ulp_above(fabs(c.t0) > fabs(c.t1) ? c.t0 : c.t1);
+    ct.reltol = c.reltol; ct.abstol = c.abstol;
+    ct.qold = QOLDINIT; ct.q11 = 1.0; ct.EEst = 1.0;
+    ct.max_steps = c.max_steps;
+    ct.active = 1;
+    ct.t_stop = c.t1;
+    if (c.form == FI_FORM_FP32) {
+        Member& m = h->mem;
+        m.dx = h->dx; m.dy = h->dy; m.A = h->dx * h->dy;
+        m.g = c.g; m.rho_ice = c.rho_ice; m.rho_litho = c.rho_litho; m.rho_um = c.rho_uppermantle;
+        m.nu = c.litho_poissonratio; m.rho_sw_ice = rsi; m.spy = c.seconds_per_year;
+        m.border_v = c.bc_viscous_border; m.border_e = c.bc_elastic_border; m.border_g = c.bc_sea_surface_border;
+        m.dt_sparse = c.dt_sparse_diagnostics;
+        m.elastic_on = elastic; m.geoid_on = geoid;
+        m.column_compressible = c.lithosphere_column == FI_COLUMN_COMPRESSIBLE;
+        m.ice_external = c.ice_mode == FI_ICE_EXTERNAL;
+        m.ice_flat = c.ice_flat_bc;
+        // FP32 parameter maps
+        std::vector<double> vf(n), sigref(n), zbss(n);
+        bool any_mask = false, any_haf = false, any_sig = false, any_ueref = false, zb_uniform = true;
+        for (size_t k = 0; k < n; k++) {
+            vf[k] = 1.0 / (2.0 * h->eta[k]);  // K / (2 eta), K == 1
+            sigref[k] = h->mask[k] * (c.rho_ice * h->H_af_ref[k] + c.rho_litho * h->ue_ref[k] +
+                                      c.rho_uppermantle * h->u_ref[k]);
+            zbss[k] = h->z_b_ref[k] - h->z_ss_ref[k] - c.z_bsl;
+            any_mask |= h->mask[k] != 1.0;
+            any_haf |= h->H_af_ref[k] != 0.0;
+            any_sig |= sigref[k] != 0.0;
+            any_ueref |= h->ue_ref[k] != 0.0;
+            zb_uniform &= zbss[k] == zbss[0];
+        }
+        m.flags = (any_mask ? FLAG_MASK : 0) | (any_haf ? FLAG_HAFREF : 0) | (any_sig ? FLAG_SIGREF : 0) |
+                  (zb_uniform ? 0 : FLAG_ZBSS) | (any_ueref ? FLAG_UEREF : 0);
+        m.zbss_scalar = (float)zbss[0];
+        RET(upload(h, (float*)m.D, h->D));
+        RET(upload(h, (float*)m.visc_fac, vf));
+        RET(upload(h, (float*)m.mask, h->mask));
+        RET(upload(h, (float*)m.H_af_ref, h->H_af_ref));
+        RET(upload(h, (float*)m.sigma_ref, sigref));
+        RET(upload(h, (float*)m.zbss_ref, zbss));
+        RET(upload(h, (float*)m.ue_ref, h->ue_ref));
+        RET(upload(h, m.ue[0], h->ue_ref));
+        if (!m.ice_external) {
+            m.K = (int)h->ice_t.size();
+            double* tt;
+            float* Ht;
+            RET(dalloc(h, &tt, m.K));
+            RET(dalloc(h, &Ht, (size_t)m.K * n));
+            RET(upload(h, tt, h->ice_t));
+            RET(upload(h, Ht, h->ice_H));
+            m.t_ice = tt;
+            m.H_tab = Ht;
+        }
+        RET(upload(h, m.u[0], u0));
+        if (elastic) RET(build_kernel_spectrum(h, h->d_Ge, (float2*)m.GA, nullptr));
+        if (geoid) RET(build_kernel_spectrum(h, h->d_Gg, (float2*)m.GB, nullptr));
+        for (int q = 0; q < 4; q++) {
+            ct.ue_corner[0][q] = ct.ue_corner[1][q] = c.bc_elastic_border;
+            ct.dz_corner[q] = c.bc_sea_surface_border;
+        }
+        CK(cudaMemcpyAsync(h->d_mem, &m, sizeof(Member), cudaMemcpyHostToDevice, h->stream));
+        RET(write_ctl(h));
+        // init_problem!: first update_diagnostics! at t0 (forces the sparse update), u <- BC(u)
+        ct.t_call = c.t0;
+        RET(write_ctl(h));
+        RET(rhs_fused(h, 1, nullptr, nullptr, nullptr));
+        CK(cudaMemcpyAsync(m.u[0], m.u[1], n * 8, cudaMemcpyDeviceToDevice, h->stream));
+        RET(read_ctl(h));
+        if (h->ctl.status) return set_err(h, h->ctl.status, "init_problem!: %s", fi_status_string(h->ctl.status));
+    } else {
+        PlainBufs& p = h->p;
+        RET(upload(h, p.D, h->D));
+        RET(upload(h, p.eta, h->eta));
+        RET(upload(h, p.mask, h->mask));
+        RET(upload(h, p.u_ref, h->u_ref));
+        RET(upload(h, p.ue_ref, h->ue_ref));
+        RET(upload(h, p.z_b_ref, h->z_b_ref));
+        RET(upload(h, p.z_ss_ref, h->z_ss_ref));
+        RET(upload(h, p.H_af_ref, h->H_af_ref));
+        if (c.ice_mode == FI_ICE_TIME_INTERPOLATED) {
+            RET(dalloc(h, &p.H_tab, h->ice_H.size()));
+            RET(upload(h, p.H_tab, h->ice_H));
+        }
+        // CurrentState(domain, ref, z_bsl)
+        RET(upload(h, p.u[0], u0));
+        RET(upload(h, p.ue, h->ue_ref));
+        RET(upload(h, p.H, h->H_ice_ref));
+        RET(upload(h, p.H_af, h->H_af_ref));
+        RET(upload(h, p.z_b, h->z_b_ref));
+        RET(upload(h, p.z_ss, h->z_ss_ref));
+        if (elastic) RET(build_kernel_spectrum(h, h->d_Ge, nullptr, p.Ge_hat));
+        if (geoid) RET(build_kernel_spectrum(h, h->d_Gg, nullptr, p.Gg_hat));
+        RET(rhs_plain(h, c.t0, p.u[0], p.fscratch));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    h->initialized = true;
+    h->last_call = 0;
+    return FI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fused form: one host-driven right-hand side (stage 0: uin -> vout/cout;
+// stage 1: state -> k1 slot), t taken from ctl.t_call
+// ---------------------------------------------------------------------------
+static int launch_sparse(fi_handle* h) {
+    k_conv_rows<<<h->n_crow, NT, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(h->d_mem, h->t_crow, h->d_plans,
+                                                                              h->h_conv);
+    CKL();
+    k_conv_cols<<<h->n_ccol, NT, conv_cols_smem(h->My, h->B_conv), h->stream>>>(h->d_mem, h->t_ccol, h->d_plans,
+                                                                              h->B_conv);
+    CKL();
+    k_conv_rows_inv<<<h->n_crowi, NT, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(h->d_mem, h->t_crowi,
+                                                                                   h->d_plans, h->h_conv);
+    CKL();
+    return FI_OK;
+}
+
+static int launch_rhs_body(fi_handle* h, int stage, const double* uin, float* vout, double* cout,
+                           cudaGraphConditionalHandle hg, cudaGraphConditionalHandle hw) {
+    k_rows_fwd<<<h->n_rows, NT, rows_fwd_smem(h->nx, h->h_rows), h->stream>>>(h->d_mem, h->t_rows, h->d_plans,
+                                                                             stage, h->h_rows, uin);
+    CKL();
+    k_cols<<<h->n_cols, NT, cols_smem(h->ny, h->B_cols), h->stream>>>(h->d_mem, h->t_cols, h->d_plans, h->B_cols);
+    CKL();
+    k_rows_inv<<<h->n_rows, NT, rows_inv_smem(h->nx, h->h_rows), h->stream>>>(h->d_mem, h->t_rows, h->d_plans,
+                                                                            stage, h->h_rows, vout, cout, hg, hw);
+    CKL();
+    return FI_OK;
+}
+
+static int rhs_fused(fi_handle* h, int stage, const double* uin, float* vout, double* cout) {
+    k_gate<<<1, 32, 0, h->stream>>>(h->d_mem, 1, h->ctl.t_call, 0);
+    CKL();
+    RET(launch_sparse(h));
+    RET(launch_rhs_body(h, stage, uin, vout, cout, 0, 0));
+    return FI_OK;
+}
+
+extern "C" int fi_rhs(fi_handle* h, double t, double* u_inout, double* dudt_out) {
+    if (!h || !u_inout || !dudt_out) return FI_ERR_ARG;
+    if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
+    const size_t n = N2(h);
+    if (h->cfg.form == FI_FORM_FP32) {
+        RET(read_ctl(h));
+        h->ctl.t_call = t;
+        h->ctl.status = FI_OK;
+        RET(write_ctl(h));
+        CK(cudaMemcpyAsync(h->d_uin, u_inout, n * 8, cudaMemcpyHostToDevice, h->stream));
+        RET(rhs_fused(h, 0, h->d_uin, h->d_vscr, h->d_cscr));
+        RET(read_ctl(h));
+        if (h->ctl.status) return set_err(h, h->ctl.status, "%s", fi_status_string(h->ctl.status));
+        std::vector<float> v(n);
+        double cc[4];
+        CK(cudaMemcpyAsync(u_inout, h->mem.u[h->ctl.ibuf ^ 1], n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(v.data(), h->d_vscr, n * 4, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(cc, h->d_cscr, 32, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const double off = corner_mean(cc) - h->cfg.bc_viscous_border;
+        for (size_t k = 0; k < n; k++) dudt_out[k] = (double)v[k] - off;
+    } else {
+        CK(cudaMemcpyAsync(h->p.uin, u_inout, n * 8, cudaMemcpyHostToDevice, h->stream));
+        RET(rhs_plain(h, t, h->p.uin, h->p.fscratch));
+        CK(cudaMemcpyAsync(u_inout, h->p.uin, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(dudt_out, h->p.fscratch, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    h->last_call = 1;
+    h->last_rhs_t = t;
+    return FI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plain FP64 form
+// ---------------------------------------------------------------------------
+static inline int gs(size_t n) { return std::max(1, std::min(4096, cdiv((long long)n, NT))); }
+
+static int corner_bc_plain(fi_handle* h, double* X, int nx, int ny, double border) {
+    kp_corner_off<<<1, 32, 0, h->stream>>>(X, nx, ny, border, h->p.off);
+    CKL();
+    kp_sub_off<<<gs((size_t)nx * ny), NT, 0, h->stream>>>(X, (size_t)nx * ny, h->p.off);
+    CKL();
+    return FI_OK;
+}
+
+static int conv_plain(fi_handle* h, const double* input, const double2* Ghat, double border, double* output) {
+    const size_t M = (size_t)h->Mx * h->My;
+    const int cx = 2 * h->nx - 1, cy = 2 * h->ny - 1;
+    PlainBufs& p = h->p;
+    k_pad_real<<<cdiv(M, NT), NT, 0, h->stream>>>(input, h->nx, h->ny, p.P, h->Mx, h->My);
+    CKL();
+    RET(fft2_64(h, p.P, h->Mx, h->My, 0));
+    kp_cmul<<<gs(M), NT, 0, h->stream>>>(p.P, Ghat, M);
+    CKL();
+    RET(fft2_64(h, p.P, h->Mx, h->My, 1));
+    kp_crop<<<gs((size_t)cx * cy), NT, 0, h->stream>>>(p.P, h->Mx, cx, cy, p.cropped);
+    CKL();
+    RET(corner_bc_plain(h, p.cropped, cx, cy, border));
+    kp_window<<<gs(N2(h)), NT, 0, h->stream>>>(p.cropped, cx, h->i1, h->j1, h->nx, h->ny, output);
+    CKL();
+    return FI_OK;
+}
+
+// update_diagnostics!(dudt, u, sim, t), one kernel per broadcast of the reference
+static int rhs_plain(fi_handle* h, double t, double* u, double* dudt) {
+    const fi_config& c = h->cfg;
+    PlainBufs& p = h->p;
+    const size_t n = N2(h);
+    const int nx = h->nx, ny = h->ny;
+    const int g = gs(n);
+    h->nf_plain += 1;
+    RET(corner_bc_plain(h, u, nx, ny, c.bc_viscous_border));
+    kp_bedrock<<<g, NT, 0, h->stream>>>(u, p.ue, p.z_b_ref, p.u_ref, p.now_u, p.z_b, p.s_m, c.rho_uppermantle, n);
+    CKL();
+    if (c.ice_mode == FI_ICE_TIME_INTERPOLATED) {
+        const std::vector<double>& tt = h->ice_t;
+        const int K = (int)tt.size();
+        int i = 0, exact = 1;
+        double dti = 1.0, ts = 0.0;
+        if (t < tt[0] || t > tt[K - 1]) {
+            if (!c.ice_flat_bc) return set_err(h, FI_ERR_FORCING_RANGE, "TimeInterpolation2D out of range.");
+            i = t < tt[0] ? 0 : K - 1;
+        } else {
+            i = (int)(std::lower_bound(tt.begin(), tt.end(), t) - tt.begin());
+            if (tt[i] != t) {
+                i -= 1;
+                exact = 0;
+                dti = tt[i + 1] - tt[i];
+                ts = t - tt[i];
+            }
+        }
+        const double* Ha = p.H_tab + (size_t)i * n;
+        const double* Hb = exact ? Ha : Ha + n;
+        kp_ice<<<g, NT, 0, h->stream>>>(Ha, Hb, dti, ts, exact, p.H, n);
+        CKL();
+    }
+    const double rsi = c.rho_seawater / c.rho_ice;
+    kp_haf_ice<<<g, NT, 0, h->stream>>>(p.H, p.z_b, p.z_ss, p.H_af_ref, p.H_af, p.s_i, rsi, c.rho_ice, n);
+    CKL();
+    if (((t - c.t0) / c.dt_sparse_diagnostics) >= (double)h->ctl.count_sparse) {
+        if (c.lithosphere == FI_LITHO_RIGID) {
+            kp_zero<<<g, NT, 0, h->stream>>>(p.ue, n);
+            CKL();
+        } else {
+            kp_copy<<<g, NT, 0, h->stream>>>(p.buf, p.s_load, n);  // columnanoms.load * K^2
+            CKL();
+            RET(conv_plain(h, p.buf, p.Ge_hat, c.bc_elastic_border, p.ue));
+        }
+        kp_litho<<<g, NT, 0, h->stream>>>(p.ue, p.ue_ref, p.s_l, c.rho_litho, n);
+        CKL();
+        if (c.sea_surface == FI_SEA_SURFACE_LATERALLY_VARIABLE) {
+            kp_geo_in<<<g, NT, 0, h->stream>>>(p.s_load, p.s_full, p.s_m, p.mask,
+                                              c.lithosphere_column == FI_COLUMN_COMPRESSIBLE, h->dx * h->dy, p.buf, n);
+            CKL();
+            RET(conv_plain(h, p.buf, p.Gg_hat, c.bc_sea_surface_border, p.dz));
+        }
+        kp_zss<<<g, NT, 0, h->stream>>>(p.z_ss_ref, p.dz, c.z_bsl, p.z_ss, n);
+        CKL();
+        kp_haf_ice<<<g, NT, 0, h->stream>>>(p.H, p.z_b, p.z_ss, p.H_af_ref, p.H_af, p.s_i, rsi, c.rho_ice, n);
+        CKL();
+        h->ctl.count_sparse += 1;
+    }
+    kp_load_full<<<g, NT, 0, h->stream>>>(p.s_i, p.s_l, p.s_m, p.mask, p.s_load, p.s_full, n);
+    CKL();
+    kp_rhs_init<<<g, NT, 0, h->stream>>>(p.s_full, c.g, p.rhs, n);
+    CKL();
+    kp_dxx<<<g, NT, 0, h->stream>>>(p.bxx, u, nx, ny, h->dx);
+    kp_dyy<<<g, NT, 0, h->stream>>>(p.byy, u, nx, ny, h->dy);
+    kp_dx<<<g, NT, 0, h->stream>>>(p.bx, u, nx, ny, h->dx);
+    kp_dy<<<g, NT, 0, h->stream>>>(p.bxy, p.bx, nx, ny, h->dy);
+    CKL();
+    kp_moments<<<g, NT, 0, h->stream>>>(p.bxx, p.byy, p.bxy, p.D, c.litho_poissonratio, p.Mxx, p.Myy, p.Mxy, n);
+    CKL();
+    kp_dxx<<<g, NT, 0, h->stream>>>(p.bxx, p.Mxx, nx, ny, h->dx);
+    kp_dyy<<<g, NT, 0, h->stream>>>(p.byy, p.Myy, nx, ny, h->dy);
+    kp_dx<<<g, NT, 0, h->stream>>>(p.bx, p.Mxy, nx, ny, h->dx);
+    kp_dy<<<g, NT, 0, h->stream>>>(p.bxy, p.bx, nx, ny, h->dy);
+    CKL();
+    kp_rhs_acc<<<g, NT, 0, h->stream>>>(p.rhs, p.bxx, p.byy, p.bxy, n);
+    kp_fftin<<<g, NT, 0, h->stream>>>(p.rhs, p.eta, p.fftrhs, n);
+    CKL();
+    RET(fft2_64(h, p.fftrhs, nx, ny, 0));
+    kp_spec<<<g, NT, 0, h->stream>>>(p.fftrhs, h->d_spinv, n);
+    CKL();
+    RET(fft2_64(h, p.fftrhs, nx, ny, 1));
+    kp_real_spy<<<g, NT, 0, h->stream>>>(p.fftrhs, c.seconds_per_year, dudt, n);
+    CKL();
+    RET(corner_bc_plain(h, dudt, nx, ny, c.bc_viscous_border));
+    kp_copy<<<g, NT, 0, h->stream>>>(p.dudt, dudt, n);
+    CKL();
+    return FI_OK;
+}
+
+static int reduce_host(fi_handle* h, const double* d_partial, int nblk, int stride, double* out) {
+    std::vector<double> v((size_t)nblk * stride);
+    CK(cudaMemcpyAsync(v.data(), d_partial, v.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int s = 0; s < stride; s++) {
+        double acc = 0.0;
+        for (int b = 0; b < nblk; b++) acc += v[(size_t)b * stride + s];
+        out[s] = acc;
+    }
+    return FI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// integrator start (OrdinaryDiffEq __init: FSAL preamble, ode_determine_initdt)
+// ---------------------------------------------------------------------------
+static int integ_start(fi_handle* h) {
+    const fi_config& c = h->cfg;
+    const size_t n = N2(h);
+    const double nd = (double)n;
+    Ctl& ct = h->ctl;
+    double d0, d1, d2 = 0.0, eqsum = 0.0;
+    double dt0;
+    const int nb = h->red_blocks;
+    if (c.form == FI_FORM_FP32) {
+        RET(read_ctl(h));
+        ct.t_call = ct.t;
+        RET(write_ctl(h));
+        // initialize!: fsalfirst = f(uprev, t)
+        RET(rhs_fused(h, 1, nullptr, nullptr, nullptr));
+        // f0 = f(u0, t) into the k4 slot
+        RET(read_ctl(h));
+        const int ik = h->ctl.ik;
+        float* f0 = h->mem.k14[ik ^ 1];
+        double* c0 = &h->d_ctl->kcorner[ik ^ 1][0];
+        RET(rhs_fused(h, 0, h->mem.u[h->ctl.ibuf], f0, c0));
+        kf_initdt_norms<<<nb, NT, 0, h->stream>>>(h->mem.u[h->ctl.ibuf], f0, c0, c.bc_viscous_border, c.abstol,
+                                                  c.reltol, h->d_red, n);
+        CKL();
+        double s[2] = {0.0, 0.0};
+        RET(reduce_host(h, h->d_red, nb, 2, s));
+        d0 = sqrt(s[0] / nd);
+        d1 = sqrt(s[1] / nd);
+        dt0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : (d0 / d1) / 100;
+        if (dt0 > ct.dtmax) dt0 = ct.dtmax;
+        if (!(dt0 < 10 * 2.220446049250313e-16)) {
+            kf_initdt_u1<<<gs(n), NT, 0, h->stream>>>(h->d_uin, h->mem.u[h->ctl.ibuf], f0, c0, c.bc_viscous_border,
+                                                      dt0, n);
+            CKL();
+            RET(read_ctl(h));
+            h->ctl.t_call = ct.t + dt0;
+            RET(write_ctl(h));
+            RET(rhs_fused(h, 0, h->d_uin, h->d_vscr, h->d_cscr));
+            kf_initdt_d2<<<nb, NT, 0, h->stream>>>(h->mem.u[h->ctl.ibuf], f0, c0, h->d_vscr, h->d_cscr,
+                                                   c.bc_viscous_border, c.abstol, c.reltol, h->d_red, n);
+            CKL();
+            RET(reduce_host(h, h->d_red, nb, 2, s));
+            d2 = sqrt(s[0] / nd) / dt0;
+            eqsum = s[1];
+        }
+        RET(read_ctl(h));
+        if (h->ctl.status) return set_err(h, h->ctl.status, "%s", fi_status_string(h->ctl.status));
+    } else {
+        PlainBufs& p = h->p;
+        RET(rhs_plain(h, ct.t, p.u[ct.ibuf], p.k14[ct.ik]));  // fsalfirst = f(uprev, t)
+        // f0 = f(u, t): the integrator's u is a separate copy of u0; sk uses u0 (already
+        // boundary-corrected, so uprev holds the same values)
+        CK(cudaMemcpyAsync(p.tmp, p.u[ct.ibuf], n * 8, cudaMemcpyDeviceToDevice, h->stream));
+        RET(rhs_plain(h, ct.t, p.tmp, p.k14[ct.ik ^ 1]));
+        kp_norms2<<<nb, NT, 0, h->stream>>>(p.tmp, p.k14[ct.ik ^ 1], p.u[ct.ibuf], c.abstol, c.reltol, p.partial, n);
+        CKL();
+        double s[2] = {0.0, 0.0};
+        RET(reduce_host(h, p.partial, nb, 2, s));
+        d0 = sqrt(s[0] / nd);
+        d1 = sqrt(s[1] / nd);
+        dt0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : (d0 / d1) / 100;
+        if (dt0 > ct.dtmax) dt0 = ct.dtmax;
+        if (!(dt0 < 10 * 2.220446049250313e-16)) {
+            kp_stage<<<gs(n), NT, 0, h->stream>>>(p.uin, p.tmp, dt0, p.k14[ct.ik ^ 1], n);
+            CKL();
+            RET(rhs_plain(h, ct.t + dt0, p.uin, p.fscratch));
+            kp_initdt_terms<<<nb, NT, 0, h->stream>>>(p.k14[ct.ik ^ 1], p.fscratch, p.u[ct.ibuf], c.abstol,
+                                                      c.reltol, p.partial, n);
+            CKL();
+            RET(reduce_host(h, p.partial, nb, 2, s));
+            d2 = sqrt(s[0] / nd) / dt0;
+            eqsum = s[1];
+        }
+    }
+    double dt;
+    if (dt0 < 10 * 2.220446049250313e-16) {
+        dt = std::max(1e-6, ct.dtmin);
+    } else if (eqsum == (double)nb * NT) {
+        dt = std::max(ct.dtmin, 100 * dt0);
+    } else {
+        const double mx = std::max(d1, d2);
+        const double dt1 = (mx <= 1e-15) ? std::max(1e-6, dt0 * 1e-3) : pow(10.0, -(2 + log10(mx)) / 3.0);
+        dt = std::max(ct.dtmin, std::min(std::min(100 * dt0, dt1), ct.dtmax));
+    }
+    if (c.form == FI_FORM_FP32) RET(read_ctl(h));
+    h->ctl.dt = dt;
+    h->ctl.dtpropose = dt;
+    h->ctl.iter = 0;
+    h->ctl.kout = 0;
+    h->fsal_pending = false;
+    if (c.form == FI_FORM_FP32) RET(write_ctl(h));
+    h->integ_started = true;
+    return FI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fused form: segment runner (CUDA graph, fallback host loop)
+// ---------------------------------------------------------------------------
+static int add_kernel(fi_handle* h, cudaGraph_t g, cudaGraphNode_t* prev, void* func, int grid, size_t smem,
+                      void** args) {
+    cudaKernelNodeParams kp{};
+    kp.func = func;
+    kp.gridDim = dim3(grid);
+    kp.blockDim = dim3(NT);
+    kp.sharedMemBytes = (unsigned)smem;
+    kp.kernelParams = args;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddKernelNode(&node, g, *prev ? prev : nullptr, *prev ? 1 : 0, &kp));
+    *prev = node;
+    return FI_OK;
+}
+
+static int add_cond(fi_handle* h, cudaGraph_t g, cudaGraphNode_t* prev, cudaGraphConditionalHandle hc,
+                    cudaGraphConditionalNodeType type, cudaGraph_t* body) {
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hc;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, *prev ? prev : nullptr, *prev ? 1 : 0, &cp));
+    *body = cp.conditional.phGraph_out[0];
+    *prev = node;
+    return FI_OK;
+}
+
+static int add_sparse(fi_handle* h, cudaGraph_t g) {
+    cudaGraphNode_t prev = nullptr;
+    const Member* mp = h->d_mem;
+    const FftPlan* pp = h->d_plans;
+    const Task *t1 = h->t_crow, *t2 = h->t_ccol, *t3 = h->t_crowi;
+    int hc = h->h_conv, bc = h->B_conv;
+    void* a1[] = {(void*)&mp, (void*)&t1, (void*)&pp, (void*)&hc};
+    RET(add_kernel(h, g, &prev, (void*)k_conv_rows, h->n_crow, conv_rows_smem(h->Mx, hc), a1));
+    void* a2[] = {(void*)&mp, (void*)&t2, (void*)&pp, (void*)&bc};
+    RET(add_kernel(h, g, &prev, (void*)k_conv_cols, h->n_ccol, conv_cols_smem(h->My, bc), a2));
+    void* a3[] = {(void*)&mp, (void*)&t3, (void*)&pp, (void*)&hc};
+    RET(add_kernel(h, g, &prev, (void*)k_conv_rows_inv, h->n_crowi, conv_rows_smem(h->Mx, hc), a3));
+    return FI_OK;
+}
+
+static int build_segment_graph(fi_handle* h) {
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    h->seg_graph = g;
+    cudaGraphConditionalHandle hw, hg[3];
+    CK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
+    for (int i = 0; i < 3; i++) CK(cudaGraphConditionalHandleCreate(&hg[i], g, 0, cudaGraphCondAssignDefault));
+    const Member* mp = h->d_mem;
+    const FftPlan* pp = h->d_plans;
+    int one = 1;
+    cudaGraphNode_t prev = nullptr;
+    {
+        void* a[] = {(void*)&mp, (void*)&one, (void*)&hg[0], (void*)&hw};
+        cudaKernelNodeParams kp{};
+        kp.func = (void*)k_segment_start;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(32);
+        kp.kernelParams = a;
+        CK(cudaGraphAddKernelNode(&prev, g, nullptr, 0, &kp));
+    }
+    cudaGraph_t body;
+    RET(add_cond(h, g, &prev, hw, cudaGraphCondTypeWhile, &body));
+    cudaGraphNode_t bp = nullptr;
+    for (int s = 2; s <= 4; s++) {
+        cudaGraph_t sb;
+        RET(add_cond(h, body, &bp, hg[s - 2], cudaGraphCondTypeIf, &sb));
+        RET(add_sparse(h, sb));
+        const Task* tr = h->t_rows;
+        const Task* tc = h->t_cols;
+        int stage = s, hr = h->h_rows, bcol = h->B_cols;
+        const double* uin = nullptr;
+        float* vout = nullptr;
+        double* cout = nullptr;
+        cudaGraphConditionalHandle hnext = (s < 4) ? hg[s - 1] : hg[0];
+        cudaGraphConditionalHandle hloop = (s == 4) ? hw : 0;
+        void* a1[] = {(void*)&mp, (void*)&tr, (void*)&pp, (void*)&stage, (void*)&hr, (void*)&uin};
+        RET(add_kernel(h, body, &bp, (void*)k_rows_fwd, h->n_rows, rows_fwd_smem(h->nx, hr), a1));
+        void* a2[] = {(void*)&mp, (void*)&tc, (void*)&pp, (void*)&bcol};
+        RET(add_kernel(h, body, &bp, (void*)k_cols, h->n_cols, cols_smem(h->ny, bcol), a2));
+        void* a3[] = {(void*)&mp, (void*)&tr, (void*)&pp, (void*)&stage, (void*)&hr,
+                      (void*)&vout, (void*)&cout, (void*)&hnext, (void*)&hloop};
+        RET(add_kernel(h, body, &bp, (void*)k_rows_inv, h->n_rows, rows_inv_smem(h->nx, hr), a3));
+    }
+    CK(cudaGraphInstantiate(&h->seg_exec, g, 0));
+    return FI_OK;
+}
+
+static int run_segment_fused(fi_handle* h) {
+    if (h->graph_ok && !h->seg_exec) {
+        if (build_segment_graph(h) != FI_OK) {
+            // conditional graph nodes unavailable: use the host loop
+            cudaGetLastError();
+            if (h->seg_graph) { cudaGraphDestroy(h->seg_graph); h->seg_graph = nullptr; }
+            h->graph_ok = false;
+        }
+    }
+    if (h->seg_exec) {
+        CK(cudaGraphLaunch(h->seg_exec, h->stream));
+        RET(read_ctl(h));
+        return FI_OK;
+    }
+    k_segment_start<<<1, 32, 0, h->stream>>>(h->d_mem, 1, 0, 0);
+    CKL();
+    const int batch = 32;
+    for (;;) {
+        for (int b = 0; b < batch; b++) {
+            for (int s = 2; s <= 4; s++) {
+                RET(launch_sparse(h));
+                RET(launch_rhs_body(h, s, nullptr, nullptr, nullptr, 0, 0));
+            }
+        }
+        RET(read_ctl(h));
+        if (!h->ctl.active) break;
+    }
+    return FI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plain form: one step attempt + host controller
+// ---------------------------------------------------------------------------
+static int attempt_plain(fi_handle* h) {
+    const fi_config& c = h->cfg;
+    PlainBufs& p = h->p;
+    Ctl& ct = h->ctl;
+    const size_t n = N2(h);
+    const double t = ct.t, dt = ct.dt;
+    double* up = p.u[ct.ibuf];
+    double* un = p.u[ct.ibuf ^ 1];
+    double* k1 = p.k14[ct.ik];
+    double* k4 = p.k14[ct.ik ^ 1];
+    kp_stage<<<gs(n), NT, 0, h->stream>>>(p.tmp, up, dt * A21, k1, n);
+    CKL();
+    RET(rhs_plain(h, t + C2 * dt, p.tmp, p.k2));
+    kp_stage<<<gs(n), NT, 0, h->stream>>>(p.tmp, up, dt * A32, p.k2, n);
+    CKL();
+    RET(rhs_plain(h, t + C3 * dt, p.tmp, p.k3));
+    kp_stage4<<<gs(n), NT, 0, h->stream>>>(un, up, dt, k1, p.k2, p.k3, n);
+    CKL();
+    RET(rhs_plain(h, t + dt, un, k4));
+    kp_err<<<h->red_blocks, NT, 0, h->stream>>>(up, un, k1, p.k2, p.k3, k4, dt, c.abstol, c.reltol, p.partial, n);
+    CKL();
+    double s = 0.0;
+    RET(reduce_host(h, p.partial, h->red_blocks, 1, &s));
+    const double EEst = sqrt(s / (double)n);
+    controller_update(&ct, EEst, h->tout.data());
+    ct.nsteps_seg += 1;
+    return FI_OK;
+}
+
+static int run_segment_plain(fi_handle* h) {
+    Ctl& ct = h->ctl;
+    ct.pending_output = 0;
+    ct.nsteps_seg = 0;
+    if (!(ct.t < ct.t_stop)) return FI_OK;
+    loopheader_prep(&ct);
+    while (ct.status == FI_OK) {
+        RET(attempt_plain(h));
+        if (ct.status != FI_OK) break;
+        if (ct.accept_step && (ct.pending_output || !(ct.t < ct.t_stop))) break;
+        loopheader_prep(&ct);
+    }
+    return FI_OK;
+}
+
+// FSAL re-evaluation after a modifying callback: k1 = f(u, t)
+static int reeval_fsal(fi_handle* h) {
+    if (h->cfg.form == FI_FORM_FP32) {
+        RET(read_ctl(h));
+        h->ctl.t_call = h->ctl.t;
+        RET(write_ctl(h));
+        RET(rhs_fused(h, 1, nullptr, nullptr, nullptr));
+        RET(read_ctl(h));
+    } else {
+        // uprev <- u (same values); f(fsalfirst, u, p, t)
+        RET(rhs_plain(h, h->ctl.t, h->p.u[h->ctl.ibuf], h->p.k14[h->ctl.ik]));
+    }
+    return FI_OK;
+}
+
+struct OutBufs {
+    double *t, *u, *ue, *dudt, *dz;
+};
+
+static int record_output(fi_handle* h, int k, const OutBufs& o) {
+    const size_t n = N2(h);
+    const fi_config& c = h->cfg;
+    if (o.t) o.t[k] = h->ctl.t;
+    if (c.form == FI_FORM_FP32) {
+        Member& m = h->mem;
+        const Ctl& ct = h->ctl;
+        if (o.u) CK(cudaMemcpyAsync(o.u + k * n, m.u[ct.ibuf], n * 8, cudaMemcpyDeviceToHost, h->stream));
+        std::vector<float> v(n);
+        if (o.ue) {
+            CK(cudaMemcpyAsync(v.data(), m.ue[ct.iue], n * 4, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            const double off = corner_mean(ct.ue_corner[ct.iue]) - c.bc_elastic_border;
+            for (size_t i = 0; i < n; i++) o.ue[k * n + i] = (double)v[i] - off;
+        }
+        if (o.dudt) {
+            CK(cudaMemcpyAsync(v.data(), m.k14[ct.ik], n * 4, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            const double off = corner_mean(ct.kcorner[ct.ik]) - c.bc_viscous_border;
+            for (size_t i = 0; i < n; i++) o.dudt[k * n + i] = (double)v[i] - off;
+        }
+        if (o.dz) {
+            CK(cudaMemcpyAsync(v.data(), m.dz, n * 4, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            const double off = corner_mean(ct.dz_corner) - c.bc_sea_surface_border;
+            for (size_t i = 0; i < n; i++) o.dz[k * n + i] = (double)v[i] - off;
+        }
+    } else {
+        PlainBufs& p = h->p;
+        if (o.u) CK(cudaMemcpyAsync(o.u + k * n, p.now_u, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        if (o.ue) CK(cudaMemcpyAsync(o.ue + k * n, p.ue, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        if (o.dudt) CK(cudaMemcpyAsync(o.dudt + k * n, p.dudt, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        if (o.dz) CK(cudaMemcpyAsync(o.dz + k * n, p.dz, n * 8, cudaMemcpyDeviceToHost, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return FI_OK;
+}
+
+// solve!(integrator): segments between tstops; outputs by nout_condition
+static int solve_until(fi_handle* h, const OutBufs* o) {
+    const bool fused = h->cfg.form == FI_FORM_FP32;
+    while (!h->tstops.empty()) {
+        if (h->fsal_pending) {
+            // apply_step! of the next attempt: reset_fsal! after a modifying callback
+            RET(reeval_fsal(h));
+            h->fsal_pending = false;
+            if (h->ctl.status != FI_OK) return set_err(h, h->ctl.status, "%s", fi_status_string(h->ctl.status));
+        }
+        if (fused) RET(read_ctl(h));
+        h->ctl.t_stop = h->tstops.front();
+        if (fused) RET(write_ctl(h));
+        if (fused) RET(run_segment_fused(h)); else RET(run_segment_plain(h));
+        Ctl& ct = h->ctl;
+        if (ct.status != FI_OK)
+            return set_err(h, ct.status, "integration stopped at t=%.6g: %s", ct.t, fi_status_string(ct.status));
+        if (ct.pending_output) {
+            if (o) RET(record_output(h, ct.kout, *o));
+            ct.kout += 1;
+            ct.pending_output = 0;
+            if (fused) RET(write_ctl(h));
+            h->fsal_pending = true;
+        }
+        while (!h->tstops.empty() && h->ctl.t == h->tstops.front()) h->tstops.erase(h->tstops.begin());
+        if (!h->tstops.empty() && h->ctl.t > h->tstops.front())
+            return set_err(h, FI_ERR_STATE, "integrator stepped past a tstop");
+    }
+    return FI_OK;
+}
+
+static int set_tstops(fi_handle* h, int n, const double* ts, bool outputs) {
+    const double t0 = h->cfg.t0, t1 = h->cfg.t1;
+    std::vector<double> v;
+    for (int i = 0; i < n; i++)
+        if (ts[i] > t0 && ts[i] <= t1) v.push_back(ts[i]);
+    v.push_back(t1);
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    h->tstops = v;
+    h->tout.assign(ts, ts + n);
+    if (n > MAX_TSTOPS) return set_err(h, FI_ERR_ARG, "too many output times");
+    h->ctl.nout = outputs ? n : 0;
+    h->ctl.kout = 0;
+    if (n) CK(cudaMemcpyAsync(h->d_tout, ts, n * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return FI_OK;
+}
+
+extern "C" int fi_run(fi_handle* h, int32_t n_out, const double* t_out, double* out_t, double* out_u,
+                      double* out_ue, double* out_dudt, double* out_dz_ss) {
+    if (!h || n_out < 0 || (n_out > 0 && !t_out)) return FI_ERR_ARG;
+    if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
+    for (int k = 1; k < n_out; k++)
+        if (t_out[k] < t_out[k - 1]) return set_err(h, FI_ERR_ARG, "t_out must be sorted");
+    RET(integ_start(h));
+    if (h->cfg.form == FI_FORM_FP32) RET(read_ctl(h));
+    RET(set_tstops(h, n_out, t_out, true));
+    if (h->cfg.form == FI_FORM_FP32) RET(write_ctl(h));
+    OutBufs o{out_t, out_u, out_ue, out_dudt, out_dz_ss};
+    RET(solve_until(h, &o));
+    h->last_call = 0;
+    return FI_OK;
+}
+
+extern "C" int fi_init_integrator(fi_handle* h, int32_t n_tstops, const double* tstops) {
+    if (!h || n_tstops < 0) return FI_ERR_ARG;
+    if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
+    RET(integ_start(h));
+    if (h->cfg.form == FI_FORM_FP32) RET(read_ctl(h));
+    // init(prob; tstops = nout.t, callback = nout_callback): the output callback still
+    // fires (and forces the FSAL re-evaluation) although nothing is recorded here
+    RET(set_tstops(h, n_tstops, tstops, true));
+    if (h->cfg.form == FI_FORM_FP32) RET(write_ctl(h));
+    return FI_OK;
+}
+
+extern "C" int fi_step(fi_handle* h, double dt) {
+    if (!h || !(dt > 0)) return FI_ERR_ARG;
+    if (!h->integ_started) return set_err(h, FI_ERR_STATE, "fi_init_integrator not called");
+    if (h->cfg.form == FI_FORM_FP32) RET(read_ctl(h));
+    const double next_t = h->ctl.t + dt;
+    if (next_t > h->cfg.t1) return set_err(h, FI_ERR_ARG, "step beyond t_span");
+    // add_tstop!(integrator, t + dt); advance until t >= next_t
+    std::vector<double>& v = h->tstops;
+    v.insert(std::lower_bound(v.begin(), v.end(), next_t), next_t);
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    std::vector<double> rest;
+    while (!v.empty() && v.back() > next_t) { rest.insert(rest.begin(), v.back()); v.pop_back(); }
+    int rc = solve_until(h, nullptr);
+    v.insert(v.end(), rest.begin(), rest.end());
+    h->last_call = 0;
+    return rc;
+}
+
+extern "C" int fi_get_stats(fi_handle* h, fi_stats* st) {
+    if (!h || !st) return FI_ERR_ARG;
+    memset(st, 0, sizeof(*st));
+    if (h->initialized) RET(read_ctl(h));
+    const Ctl& ct = h->ctl;
+    st->t = ct.t;
+    st->dt = ct.dtpropose;
+    st->nf = h->cfg.form == FI_FORM_FP32 ? ct.nf : h->nf_plain;
+    st->naccept = ct.naccept;
+    st->nreject = ct.nreject;
+    st->nsparse = ct.count_sparse;
+    st->status = ct.status;
+    st->form = h->cfg.form;
+    return FI_OK;
+}
+
+extern "C" int fi_get_field(fi_handle* h, int32_t field, double* host, size_t n) {
+    if (!h || !host) return FI_ERR_ARG;
+    if (n != N2(h)) return set_err(h, FI_ERR_ARG, "field size %zu != nx*ny", n);
+    std::vector<double> v;
+    const fi_config& c = h->cfg;
+    const bool fused = c.form == FI_FORM_FP32;
+    switch (field) {
+        case FI_FIELD_LITHO_RIGIDITY: v = h->D; break;
+        case FI_FIELD_EFFECTIVE_VISCOSITY: v = h->eta; break;
+        case FI_FIELD_MASKACTIVE: v = h->mask; break;
+        case FI_FIELD_U_REF: v = h->u_ref; break;
+        case FI_FIELD_UE_REF: v = h->ue_ref; break;
+        case FI_FIELD_DZ_SS_REF: v = h->dz_ss_ref; break;
+        case FI_FIELD_Z_B_REF: v = h->z_b_ref; break;
+        case FI_FIELD_PSEUDODIFF_SCALING: RET(download(h, v, h->d_R, n)); break;
+        case FI_FIELD_PSEUDODIFF: RET(download(h, v, h->d_pd, n)); break;
+        case FI_FIELD_SCALED_PSEUDODIFF_INV: RET(download(h, v, h->d_spinv, n)); break;
+        case FI_FIELD_ELASTIC_GREEN: RET(download(h, v, h->d_Ge, n)); break;
+        case FI_FIELD_DZ_SS_GREEN: RET(download(h, v, h->d_Gg, n)); break;
+        default: {
+            if (!h->initialized) return set_err(h, FI_ERR_STATE, "state fields need fi_init");
+            RET(read_ctl(h));
+            const Ctl& ct = h->ctl;
+            if (!fused) {
+                const PlainBufs& p = h->p;
+                const double* src = nullptr;
+                switch (field) {
+                    case FI_FIELD_U: src = p.now_u; break;
+                    case FI_FIELD_UE: src = p.ue; break;
+                    case FI_FIELD_DUDT: src = p.dudt; break;
+                    case FI_FIELD_DZ_SS: src = p.dz; break;
+                    case FI_FIELD_H_ICE: src = p.H; break;
+                    case FI_FIELD_Z_SS: src = p.z_ss; break;
+                    case FI_FIELD_Z_B: src = p.z_b; break;
+                    case FI_FIELD_COLUMNANOM_LOAD: src = p.s_load; break;
+                    case FI_FIELD_COLUMNANOM_FULL: src = p.s_full; break;
+                    case FI_FIELD_H_AF: src = p.H_af; break;
+                    default: return set_err(h, FI_ERR_ARG, "unknown field %d", field);
+                }
+                RET(download(h, v, src, n));
+                break;
+            }
+            const Member& m = h->mem;
+            std::vector<double> ue, dz;
+            RET(download(h, ue, m.ue[ct.iue], n));
+            const double cue = corner_mean(ct.ue_corner[ct.iue]) - c.bc_elastic_border;
+            for (auto& x : ue) x -= cue;
+            RET(download(h, dz, m.dz, n));
+            const double cdz = corner_mean(ct.dz_corner) - c.bc_sea_surface_border;
+            for (auto& x : dz) x -= cdz;
+            switch (field) {
+                case FI_FIELD_U: RET(download(h, v, m.u[h->last_call == 1 ? ct.ibuf ^ 1 : ct.ibuf], n)); break;
+                case FI_FIELD_UE: v = ue; break;
+                case FI_FIELD_DZ_SS: v = dz; break;
+                case FI_FIELD_DUDT: {
+                    const bool scr = h->last_call == 1;
+                    RET(download(h, v, scr ? h->d_vscr : m.k14[ct.ik], n));
+                    double cc[4];
+                    if (scr) {
+                        CK(cudaMemcpy(cc, h->d_cscr, 32, cudaMemcpyDeviceToHost));
+                    } else {
+                        memcpy(cc, ct.kcorner[ct.ik], 32);
+                    }
+                    const double off = corner_mean(cc) - c.bc_viscous_border;
+                    for (auto& x : v) x -= off;
+                    break;
+                }
+                case FI_FIELD_H_ICE: {
+                    int st;
+                    interp_ice_host(h, h->last_call == 1 ? h->last_rhs_t : ct.t, v, &st);
+                    if (c.ice_mode == FI_ICE_EXTERNAL) RET(download(h, v, m.H_ext, n));
+                    break;
+                }
+                case FI_FIELD_Z_SS:
+                    v.resize(n);
+                    for (size_t k = 0; k < n; k++) v[k] = h->z_ss_ref[k] + dz[k] + c.z_bsl;
+                    break;
+                case FI_FIELD_COLUMNANOM_LOAD: RET(download(h, v, m.sig_load, n)); break;
+                case FI_FIELD_COLUMNANOM_FULL:
+                    if (m.column_compressible) return set_err(h, FI_ERR_UNSUPPORTED, "full anomaly not kept");
+                    RET(download(h, v, m.sig_geo, n));
+                    for (auto& x : v) x /= m.A;
+                    break;
+                default: return set_err(h, FI_ERR_ARG, "field %d not available in the FP32 form", field);
+            }
+        }
+    }
+    memcpy(host, v.data(), n * sizeof(double));
+    return FI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// checkpoint / restore: control block + every state buffer
+// ---------------------------------------------------------------------------
+struct Blob {
+    void* d;
+    size_t bytes;
+};
+
+static std::vector<Blob> state_blobs(fi_handle* h) {
+    const size_t n = N2(h);
+    std::vector<Blob> b;
+    if (h->cfg.form == FI_FORM_FP32) {
+        Member& m = h->mem;
+        for (int i = 0; i < 2; i++) {
+            b.push_back({m.u[i], n * 8});
+            b.push_back({m.k14[i], n * 4});
+            b.push_back({m.ue[i], n * 4});
+        }
+        b.push_back({m.k2, n * 4});
+        b.push_back({m.k3, n * 4});
+        b.push_back({m.dz, n * 4});
+        b.push_back({m.sig_load, n * 4});
+        b.push_back({m.sig_geo, n * 4});
+        b.push_back({m.H_ext, n * 4});
+    } else {
+        PlainBufs& p = h->p;
+        double* bufs[] = {p.u[0], p.u[1], p.k14[0], p.k14[1], p.k2, p.k3, p.now_u, p.ue, p.dz, p.H, p.H_af, p.z_b,
+                          p.z_ss, p.s_i, p.s_l, p.s_m, p.s_load, p.s_full, p.dudt};
+        for (double* q : bufs) b.push_back({q, n * 8});
+    }
+    return b;
+}
+
+extern "C" int fi_checkpoint(fi_handle* h, void* buf, size_t* size) {
+    if (!h || !size) return FI_ERR_ARG;
+    if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
+    auto blobs = state_blobs(h);
+    size_t need = sizeof(Ctl) + sizeof(long long) + sizeof(int) + sizeof(double) * (1 + h->tstops.size());
+    for (auto& b : blobs) need += b.bytes;
+    if (!buf) { *size = need; return FI_OK; }
+    if (*size < need) return set_err(h, FI_ERR_ARG, "checkpoint buffer too small");
+    RET(read_ctl(h));
+    char* w = (char*)buf;
+    memcpy(w, &h->ctl, sizeof(Ctl)); w += sizeof(Ctl);
+    memcpy(w, &h->nf_plain, sizeof(long long)); w += sizeof(long long);
+    int ls = h->last_call;
+    memcpy(w, &ls, sizeof(int)); w += sizeof(int);
+    double nts = (double)h->tstops.size();
+    memcpy(w, &nts, sizeof(double)); w += sizeof(double);
+    memcpy(w, h->tstops.data(), h->tstops.size() * sizeof(double)); w += h->tstops.size() * sizeof(double);
+    for (auto& b : blobs) {
+        CK(cudaMemcpyAsync(w, b.d, b.bytes, cudaMemcpyDeviceToHost, h->stream));
+        w += b.bytes;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    *size = need;
+    return FI_OK;
+}
+
+extern "C" int fi_restore(fi_handle* h, const void* buf, size_t size) {
+    if (!h || !buf) return FI_ERR_ARG;
+    if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init must precede fi_restore");
+    const char* r = (const char*)buf;
+    if (size < sizeof(Ctl) + sizeof(long long) + sizeof(int) + sizeof(double))
+        return set_err(h, FI_ERR_ARG, "checkpoint too small");
+    memcpy(&h->ctl, r, sizeof(Ctl)); r += sizeof(Ctl);
+    memcpy(&h->nf_plain, r, sizeof(long long)); r += sizeof(long long);
+    int ls;
+    memcpy(&ls, r, sizeof(int)); r += sizeof(int);
+    h->last_call = ls;
+    double nts;
+    memcpy(&nts, r, sizeof(double)); r += sizeof(double);
+    h->tstops.assign((const double*)r, (const double*)r + (size_t)nts);
+    r += (size_t)nts * sizeof(double);
+    auto blobs = state_blobs(h);
+    size_t need = (size_t)(r - (const char*)buf);
+    for (auto& b : blobs) need += b.bytes;
+    if (size < need) return set_err(h, FI_ERR_ARG, "checkpoint size mismatch");
+    for (auto& b : blobs) {
+        CK(cudaMemcpyAsync(b.d, r, b.bytes, cudaMemcpyHostToDevice, h->stream));
+        r += b.bytes;
+    }
+    RET(write_ctl(h));
+    CK(cudaStreamSynchronize(h->stream));
+    h->integ_started = true;
+    return FI_OK;
+}

@@ -1,0 +1,52 @@
+// fi_kernels.h -- kernel declarations shared by the translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fi_internal.cuh"
+
+namespace fi {
+
+// ---- fused FP32 form (fi_fused.cu) ----
+__global__ void k_gate(const Member* mems, int nmem, double t, int use_ctl_t);
+__global__ void k_rows_fwd(const Member* mems, const Task* tasks, const FftPlan* plans, int stage, int h,
+                           const double* uin);
+__global__ void k_cols(const Member* mems, const Task* tasks, const FftPlan* plans, int B);
+__global__ void k_rows_inv(const Member* mems, const Task* tasks, const FftPlan* plans, int stage, int h,
+                           float* vout, double* cout, cudaGraphConditionalHandle h_gate,
+                           cudaGraphConditionalHandle h_loop);
+__global__ void k_conv_rows(const Member* mems, const Task* tasks, const FftPlan* plans, int h);
+__global__ void k_conv_cols(const Member* mems, const Task* tasks, const FftPlan* plans, int B);
+__global__ void k_conv_rows_inv(const Member* mems, const Task* tasks, const FftPlan* plans, int h);
+__global__ void k_segment_start(const Member* mems, int nmem, cudaGraphConditionalHandle h_gate,
+                                cudaGraphConditionalHandle h_loop);
+__global__ void kf_initdt_norms(const double* u, const float* v, const double* vc, double border, double abstol,
+                                double reltol, double* partial, size_t n);
+__global__ void kf_initdt_u1(double* u1, const double* u, const float* v, const double* vc, double border,
+                             double dt0, size_t n);
+__global__ void kf_initdt_d2(const double* u, const float* v0, const double* c0p, const float* v1,
+                             const double* c1p, double border, double abstol, double reltol, double* partial,
+                             size_t n);
+size_t rows_fwd_smem(int nx, int h);
+size_t cols_smem(int ny, int B);
+size_t rows_inv_smem(int nx, int h);
+size_t conv_rows_smem(int Mx, int h);
+size_t conv_cols_smem(int My, int B);
+
+// ---- FP64 transforms and set-up (fi_setup.cu) ----
+__global__ void k_fft64_rows(double2* a, int nx, int ny, int pitch, const FftPlan* plans, int plan, int inverse,
+                             int rows_per_block);
+__global__ void k_fft64_cols(double2* a, int nx, int ny, int pitch, const FftPlan* plans, int plan, int inverse,
+                             int cols_per_block, double scale);
+size_t fft64_rows_smem(int nx, int rows_per_block);
+size_t fft64_cols_smem(int ny, int cols_per_block);
+__global__ void k_spectral_factors(int nx, int ny, double Wx, double Wy, int nch, const double* ratio,
+                                   const double* thick, const double* R_given, double spy, double* pseudodiff,
+                                   double* Rout, double* spinv, float* mult, int NH);
+__global__ void k_elastic_green(double* G, int nx, int ny, int mx, int my, double dx, double dy, const double* rm,
+                                const double* GE, int n);
+__global__ void k_geoid_green(double* G, int nx, int ny, double Wx, double Wy, double dx, double dy,
+                              double r_pole, double mE);
+__global__ void k_pad_real(const double* in, int nx, int ny, double2* P, int Mx, int My);
+__global__ void k_half_spectrum32(const double2* P, int Mx, int My, int MH, double scale, float2* out);
+
+}  // namespace fi

@@ -1,0 +1,200 @@
+/*
+ * fastiso_b200.h -- C ABI of the B200-native LV-ELVA hot path of FastIsostasy.jl.
+ *
+ * The library replaces the laterally-variable ELVA (elastic lithosphere, viscous
+ * asthenosphere) right-hand side and the adaptive BS3 integrator that drives it:
+ *
+ *   update_diagnostics!(dudt, u, sim, t)          src/simulation.jl:335-393
+ *   update_dudt!(.., ::MaxwellMantle, ::LaterallyVariableLithosphere)
+ *                                                 src/deformation.jl:91-103
+ *   update_deformation_rhs!                       src/deformation.jl:110-131
+ *   update_elasticresponse!                       src/deformation.jl:175-184
+ *   update_dz_ss!(::LaterallyVariableSeaSurface)  src/sealevel.jl:173-201
+ *   samesize_conv!/conv!                          src/convolutions.jl:94-154
+ *   run!(sim) -> solve(prob, BS3(); reltol)       src/simulation.jl:236-262
+ *   init_integrator / step!(integrator, dt, true) src/simulation.jl:293-322
+ *
+ * All arrays crossing this boundary are host arrays of double in the Julia
+ * column-major layout of the reference (element (i,j) at i + j*nx, x fastest,
+ * dimension 1 = x; test/test_dimensions.jl:14-19).  The caller owns every host
+ * buffer; each call copies in or out and keeps no pointer past its return.
+ * The library owns its device memory, streams and CUDA graphs for the lifetime
+ * of a handle.  A handle is not thread-safe; distinct handles may be used from
+ * distinct host threads.  Every entry point returns FI_OK (0) or an FI_ERR_*
+ * code; fi_last_error() returns the message of the last failure on a handle.
+ */
+#ifndef FASTISO_B200_H
+#define FASTISO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FI_ABI_VERSION 1
+
+/* ---- status codes (error(...) calls of the reference become these) ---- */
+enum {
+    FI_OK = 0,
+    FI_ERR_ARG = 1,            /* invalid argument or size */
+    FI_ERR_CUDA = 2,           /* CUDA runtime error */
+    FI_ERR_NONFINITE = 3,      /* NaN/Inf in the error norm or state */
+    FI_ERR_DT_UNDERFLOW = 4,   /* adaptive dt fell below dtmin */
+    FI_ERR_FORCING_RANGE = 5,  /* "TimeInterpolation2D out of range." (src/interpolations.jl:51-58) */
+    FI_ERR_TIMEOUT = 6,        /* a bounded device wait gave up */
+    FI_ERR_STATE = 7,          /* call out of lifecycle order */
+    FI_ERR_UNSUPPORTED = 8,    /* option outside the LV-ELVA path */
+    FI_ERR_MAXITERS = 9        /* step budget exhausted */
+};
+
+/* ---- compute form ---- */
+enum {
+    FI_FORM_FP32 = 0,  /* fused kernels: FP32 FFTs, stencils and spectral multiplies,
+                          FP64 state, first stencil and controller; CUDA graph */
+    FI_FORM_FP64 = 1   /* plain form: one FP64 kernel per operation, host-driven loop */
+};
+
+/* ---- tags of the reference (src/solidearth.jl:13-109, src/sealevel.jl:114-130) ---- */
+enum { FI_LITHO_LATERALLY_VARIABLE = 0, FI_LITHO_RIGID = 1 };
+enum { FI_SEA_SURFACE_LATERALLY_CONSTANT = 0, FI_SEA_SURFACE_LATERALLY_VARIABLE = 1 };
+enum { FI_COLUMN_INCOMPRESSIBLE = 0, FI_COLUMN_COMPRESSIBLE = 1 };
+enum { FI_ICE_TIME_INTERPOLATED = 0, FI_ICE_EXTERNAL = 1 };
+
+/* Scalars of RegionalDomain, PhysicalConstants, SolidEarth, RegionalSeaLevel and
+ * SolverOptions that the hot path reads.  fi_config_default() fills the
+ * reference defaults (src/constants.jl:16-28, src/solidearth.jl:115-121,
+ * src/simulation.jl:11-26). */
+typedef struct fi_config {
+    int32_t nx, ny;                 /* RegionalDomain(Wx, Wy, nx, ny), src/domain.jl:76 */
+    double Wx, Wy;                  /* half-widths (m) */
+    /* PhysicalConstants */
+    double mE, r_pole, g, seconds_per_year;
+    double rho_ice, rho_water, rho_seawater;
+    /* SolidEarth scalars */
+    double rho_litho, rho_uppermantle, litho_poissonratio;
+    int32_t lithosphere;            /* FI_LITHO_* (Rigid => ue = 0, deformation.jl:186-189) */
+    int32_t lithosphere_column;     /* FI_COLUMN_* (sealevel.jl:193-201) */
+    /* RegionalSeaLevel with ConstantBSL and NoSealevelLoad */
+    int32_t sea_surface;            /* FI_SEA_SURFACE_* */
+    double z_bsl;                   /* ConstantBSL level (m) */
+    /* boundary conditions: BoundaryConditions(...) x_border of the three CornerBCs */
+    double bc_viscous_border, bc_elastic_border, bc_sea_surface_border;
+    int32_t ice_mode;               /* FI_ICE_* */
+    int32_t ice_flat_bc;            /* TimeInterpolation2D flat_bc */
+    /* SolverOptions / DiffEqOptions */
+    double t0, t1;                  /* t_span */
+    double reltol, abstol;          /* reltol = Float64(1f-5), abstol = 1e-6 */
+    double dt_sparse_diagnostics;   /* 10 yr */
+    int64_t max_steps;              /* step-attempt budget per run/step call (0 = unlimited) */
+    int32_t form;                   /* FI_FORM_* */
+    int32_t reserved;
+} fi_config;
+
+/* Fields addressable by fi_set_field / fi_get_field.  All are nx*ny doubles. */
+enum {
+    FI_FIELD_LITHO_RIGIDITY = 0,      /* SolidEarth.litho_rigidity D (set, required) */
+    FI_FIELD_EFFECTIVE_VISCOSITY = 1, /* SolidEarth.effective_viscosity (set, required) */
+    FI_FIELD_PSEUDODIFF_SCALING = 2,  /* SolidEarth.pseudodiff_scaling R, spectral index
+                                         (set optional; default from channel layers or 1) */
+    FI_FIELD_MASKACTIVE = 3,          /* SolidEarth.maskactive as 0/1 (set optional) */
+    FI_FIELD_U_REF = 4,               /* Simulation(...; u_ref) */
+    FI_FIELD_UE_REF = 5,              /* Simulation(...; ue_ref) */
+    FI_FIELD_DZ_SS_REF = 6,           /* Simulation(...; dz_ss_ref) */
+    FI_FIELD_Z_B_REF = 7,             /* Simulation(...; z_b_ref), default 1e6 */
+    FI_FIELD_U = 8,                   /* sim.now.u (get; set before fi_init overrides u_ref copy) */
+    FI_FIELD_UE = 9,                  /* sim.now.ue */
+    FI_FIELD_DUDT = 10,               /* sim.now.dudt */
+    FI_FIELD_DZ_SS = 11,              /* sim.now.dz_ss */
+    FI_FIELD_H_ICE = 12,              /* sim.now.H_ice (set for FI_ICE_EXTERNAL) */
+    FI_FIELD_Z_SS = 13,               /* sim.now.z_ss */
+    FI_FIELD_Z_B = 14,                /* sim.now.z_b */
+    FI_FIELD_ELASTIC_GREEN = 15,      /* GIATools elastic Green's function (get) */
+    FI_FIELD_DZ_SS_GREEN = 16,        /* GIATools sea-surface Green's function (get) */
+    FI_FIELD_PSEUDODIFF = 17,         /* RegionalDomain.pseudodiff (get) */
+    FI_FIELD_SCALED_PSEUDODIFF_INV = 18, /* SolidEarth.scaled_pseudodiff_inv (get) */
+    FI_FIELD_COLUMNANOM_LOAD = 19,    /* sim.now.columnanoms.load (get) */
+    FI_FIELD_COLUMNANOM_FULL = 20,    /* sim.now.columnanoms.full (get) */
+    FI_FIELD_H_AF = 21,               /* sim.now.H_af (get) */
+    FI_NUM_FIELDS = 22
+};
+
+typedef struct fi_stats {
+    double t;                 /* integrator time (yr) */
+    double dt;                /* proposed next dt (yr) */
+    int64_t nf;               /* RHS evaluations (update_diagnostics! calls) */
+    int64_t naccept, nreject; /* step attempts */
+    int64_t nsparse;          /* sparse elastic / sea-surface updates (count_sparse_updates) */
+    int32_t status;           /* FI_OK or the device status code */
+    int32_t form;
+} fi_stats;
+
+typedef struct fi_handle fi_handle;
+
+/* Fill cfg with the reference defaults for a domain of 2Wx x 2Wy and nx x ny cells. */
+void fi_config_default(fi_config* cfg, int32_t nx, int32_t ny, double Wx, double Wy);
+
+/* Simulation(domain, bcs, sealevel, solidearth, t_span; ...) -- src/simulation.jl:105-156.
+ * Allocates device state; fields are set afterwards. */
+int fi_create(const fi_config* cfg, fi_handle** out);
+
+/* Copy a host field (nx*ny doubles) to / from the device. */
+int fi_set_field(fi_handle* h, int32_t field, const double* host, size_t n);
+int fi_get_field(fi_handle* h, int32_t field, double* host, size_t n);
+
+/* TimeInterpolatedIceThickness(t_vec, H_vec, domain) -- src/boundary_conditions.jl:36-40.
+ * K snapshots, H is K*nx*ny doubles, t strictly increasing. */
+int fi_set_ice_history(fi_handle* h, int32_t K, const double* t, const double* H);
+
+/* get_greenintegrand_coeffs -> build_greenintegrand -> get_elastic_green
+ * (src/dataloaders.jl:257-273, src/material.jl:299-364, src/tools.jl:64-71):
+ * the elastic Green's function is integrated in FP64 on the device from the
+ * Farrell (1972) table (distance rm in m, coefficients GE), n entries. */
+int fi_set_elastic_table(fi_handle* h, int32_t n, const double* rm, const double* GE);
+
+/* FreqDomainViscosityLumping channel scaling (src/material.jl:154-179, 232-278):
+ * n channels, each with its mask-mean viscosity ratio and mean thickness (m).
+ * R(|k|) is evaluated in FP64 on the device.  Without this call (or a
+ * FI_FIELD_PSEUDODIFF_SCALING field) R = 1, the one-layer case. */
+int fi_set_channel_scaling(fi_handle* h, int32_t n, const double* visc_ratio_mean,
+                           const double* channel_thickness_mean);
+
+/* Reference state + init_problem! (src/simulation.jl:129-156, 305-312): builds the
+ * Green's functions and spectral factors, the reference state, and performs the
+ * first RHS evaluation (which forces the sparse update). */
+int fi_init(fi_handle* h);
+
+/* One update_diagnostics!(dudt, u, sim, t) call with all its side effects on the
+ * state (sparse update gate, column anomalies).  u is modified in place by the
+ * viscous corner boundary condition exactly as in the reference. */
+int fi_rhs(fi_handle* h, double t, double* u_inout, double* dudt_out);
+
+/* run!(sim) with NativeOutput times t_out (src/simulation.jl:236-262): integrates
+ * t0 -> t1 with BS3 and the reference tolerances; at each output (same callback
+ * semantics as nout_condition/nout_affect!) copies u, ue, dudt and dz_ss into
+ * out_* (n_out*nx*ny each, any may be NULL) and the output time into out_t. */
+int fi_run(fi_handle* h, int32_t n_out, const double* t_out, double* out_t,
+           double* out_u, double* out_ue, double* out_dudt, double* out_dz_ss);
+
+/* init_integrator(sim) (src/simulation.jl:293-303) with tstops; then
+ * fi_step(h, dt) = step!(integrator, dt, true) (src/simulation.jl:319-322). */
+int fi_init_integrator(fi_handle* h, int32_t n_tstops, const double* tstops);
+int fi_step(fi_handle* h, double dt);
+
+/* Counters of the integrator and the RHS. */
+int fi_get_stats(fi_handle* h, fi_stats* st);
+
+/* Checkpoint: the full integrator + diagnostic state.  fi_checkpoint with
+ * buf == NULL writes the needed size into *size. */
+int fi_checkpoint(fi_handle* h, void* buf, size_t* size);
+int fi_restore(fi_handle* h, const void* buf, size_t size);
+
+const char* fi_last_error(const fi_handle* h);
+const char* fi_status_string(int32_t status);
+void fi_destroy(fi_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASTISO_B200_H */

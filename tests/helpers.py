@@ -1,0 +1,46 @@
+"""Test helpers: build a library simulation and the oracle (the checker) from the same
+host-side inputs, and compare fields."""
+from __future__ import annotations
+
+import numpy as np
+
+import fastiso_b200 as F
+from fastiso_b200 import abi
+from oracle import oracle as O
+
+
+def F_(a):
+    """numpy (nx, ny) -> flat x-fastest buffer"""
+    return np.asarray(a, dtype=np.float64).ravel(order="F")
+
+
+def oracle_for(sim: F.Simulation) -> O.OracleSim:
+    inp = sim.prepared_inputs()
+    ref = O.OracleSim(inp["cfg"])
+    for name, arr in inp["fields"].items():
+        ref.set_field(abi.FIELDS[name], F_(arr))
+    if inp["ice_t"] is not None:
+        ref.set_ice_history(inp["ice_t"], np.stack([F_(h) for h in inp["ice_H"]]))
+    ref.set_elastic_table(*inp["elastic_table"])
+    ratio, thick = inp["channels"]
+    if ratio.size:
+        ref.set_channel_scaling(ratio, thick)
+    return ref
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+#: one right-hand side on identical inputs (dudt, ue, dz_ss): kernel-level parity
+TOL = {"fp64": 1e-10, "fp32": 1e-6}
+#: displacement over a run at the reference tolerance (reltol = Float64(1f-5)); the
+#: adaptive step sequence amplifies round-off, so two correct runs differ by up to the
+#: integrator's own error (about 6e-4 against a tight-tolerance solution here)
+RUN_TOL = {"fp64": 1e-6, "fp32": 2e-3}
+#: sparse diagnostics (ue, dz_ss) are sampled at stage times every 10 yr and are more
+#: sensitive to the step sequence
+RUN_TOL_SPARSE = {"fp64": 2e-3, "fp32": 5e-3}

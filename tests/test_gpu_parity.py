@@ -1,0 +1,229 @@
+"""GPU parity: libfastiso_b200.so (through its C ABI) against the FP64 oracle on the
+same seeded inputs.  Tolerances (rel-L2): plain FP64 form 1e-10 per right-hand side
+and 1e-8 per run; fused FP32 form 1e-4."""
+import numpy as np
+import pytest
+
+import fastiso_b200 as F
+import fastiso_b200.workloads as W
+from fastiso_b200 import abi
+from helpers import F_, TOL, RUN_TOL, RUN_TOL_SPARSE, oracle_for, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FORMS = ["fp64", "fp32"]
+
+
+def small_sim(form, nx=32, ny=32, W_=0.75e6, t_end=2000.0, sea_surface=True, litho="lv", column="inc",
+              refs=False, mask=False, layers=1, external=False, seed=0):
+    domain = F.RegionalDomain(W_, W_ * ny / nx, nx, ny)
+    rng = np.random.default_rng(seed)
+    log10eta = 21 + 0.5 * np.exp(-domain.R**2 / (2 * (W_ / 4) ** 2)) + 0.1 * rng.standard_normal((nx, ny))
+    T = 100e3 + 20e3 * rng.random((nx, ny))
+    if layers == 1:
+        se_kw = dict(layer_boundaries=T.reshape(nx, ny, 1), layer_viscosities=(10**log10eta).reshape(nx, ny, 1))
+    else:
+        lb = np.stack([T, T + 150e3], axis=2)
+        lv = np.stack([10 ** (log10eta - 1), 10**log10eta], axis=2)
+        se_kw = dict(layer_boundaries=lb, layer_viscosities=lv)
+    maskactive = (domain.R < 0.8 * W_) if mask else None
+    se = F.SolidEarth(domain, maskactive=maskactive,
+                      lithosphere=F.RigidLithosphere() if litho == "rigid" else F.LaterallyVariableLithosphere(),
+                      lithosphere_column=F.CompressibleLithosphereColumn() if column == "comp"
+                      else F.IncompressibleLithosphereColumn(), **se_kw)
+    H1 = 1e3 * (domain.R < 0.4 * W_)
+    if external:
+        it = F.ExternallyUpdatedIceThickness()
+    else:
+        it = F.TimeInterpolatedIceThickness([0.0, 1.0, t_end], [domain.zeros(), H1, 1.3 * H1], domain)
+    bcs = F.BoundaryConditions(domain, ice_thickness=it)
+    sl = F.RegionalSeaLevel(surface=F.LaterallyVariableSeaSurface() if sea_surface else F.LaterallyConstantSeaSurface())
+    kw = {}
+    if refs:
+        kw = dict(u_ref=5 * rng.standard_normal((nx, ny)), ue_ref=0.5 * rng.standard_normal((nx, ny)),
+                  z_b_ref=100 * rng.standard_normal((nx, ny)))
+    return F.Simulation(domain, bcs, sl, se, (0.0, t_end), form=form, **kw)
+
+
+def pair(sim):
+    ref = oracle_for(sim)
+    ref.init()
+    sim.init_problem()
+    return ref
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_setup_fields(form):
+    sim = small_sim(form, 24, 20, layers=2)
+    ref = pair(sim)
+    for name in ("pseudodiff", "scaled_pseudodiff_inv", "pseudodiff_scaling", "elastic_green", "dz_ss_green"):
+        got = F_(sim.get_field(name))
+        want = ref.get_field(abi.FIELDS[name])
+        assert rel_l2(got, want) < 1e-12, name
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("shape", [(16, 16), (17, 15), (64, 64), (96, 96), (30, 50)])
+def test_rhs_parity(form, shape):
+    nx, ny = shape
+    sim = small_sim(form, nx, ny, t_end=100.0)
+    ref = pair(sim)
+    rng = np.random.default_rng(1)
+    u = -50 * np.exp(-sim.domain.R**2 / (2 * (0.3 * sim.domain.Wx) ** 2)) + 0.5 * rng.standard_normal((nx, ny))
+    for t in (0.5, 3.0, 12.5, 12.7, 31.0):
+        ug, dg = u.copy(), np.zeros_like(u)
+        F.update_diagnostics(dg, ug, sim, t)
+        ur, dr = ref.rhs(t, F_(u))
+        assert rel_l2(F_(ug), ur) < 1e-12
+        assert rel_l2(F_(dg), dr) < TOL[form], (t, rel_l2(F_(dg), dr))
+        assert rel_l2(F_(sim.get_field("ue")), ref.get_field(abi.FIELDS["ue"])) < TOL[form]
+        assert rel_l2(F_(sim.get_field("dz_ss")), ref.get_field(abi.FIELDS["dz_ss"])) < TOL[form]
+        u = u + 0.1 * dg
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("variant", ["rigid", "compressible", "refs_mask", "no_geoid", "two_layers"])
+def test_rhs_variants(form, variant):
+    kw = {"rigid": dict(litho="rigid"), "compressible": dict(column="comp"), "refs_mask": dict(refs=True, mask=True),
+          "no_geoid": dict(sea_surface=False), "two_layers": dict(layers=2)}[variant]
+    sim = small_sim(form, 24, 24, t_end=100.0, **kw)
+    ref = pair(sim)
+    u = -30 * np.exp(-sim.domain.R**2 / (2 * (0.3 * sim.domain.Wx) ** 2))
+    for t in (0.5, 11.0, 25.0):
+        ug, dg = u.copy(), np.zeros_like(u)
+        F.update_diagnostics(dg, ug, sim, t)
+        ur, dr = ref.rhs(t, F_(u))
+        assert rel_l2(F_(dg), dr) < TOL[form], (variant, t, rel_l2(F_(dg), dr))
+        u = u + 0.1 * dg
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_run_parity_small(form):
+    """run! against the oracle at the reference tolerance, and both against a
+    tight-tolerance oracle run (the true solution): the library must be as close to
+    the truth as the reference's own run is."""
+    tout = [0.0, 500.0, 1000.0, 2000.0]
+    sim = small_sim(form, 32, 32, t_end=2000.0)
+    sim.nout.t = tout
+    ref = pair(sim)
+    F.run(sim)
+    out = ref.run(np.asarray(tout))
+    tight = small_sim("fp64", 32, 32, t_end=2000.0)
+    tight.cfg.reltol, tight.cfg.abstol = 1e-8, 1e-10
+    rt = oracle_for(tight)
+    rt.init()
+    truth = rt.run(np.asarray(tout), want=("u",))
+    print(form, sim.stats(), ref.stats())
+    for k in range(len(tout)):
+        for var in ("u", "dudt"):
+            e = rel_l2(F_(sim.nout.out[var][k]), out[var][k])
+            assert e < RUN_TOL[form] * (10 if var == "dudt" else 1), (form, k, var, e)
+        for var in ("ue", "dz_ss"):
+            e = rel_l2(F_(sim.nout.out[var][k]), out[var][k])
+            assert e < RUN_TOL_SPARSE[form], (form, k, var, e)
+        if k > 0:
+            e_lib = rel_l2(F_(sim.nout.out["u"][k]), truth["u"][k])
+            e_ref = rel_l2(out["u"][k], truth["u"][k])
+            assert e_lib <= 3 * e_ref + 2e-4, (form, k, e_lib, e_ref)
+    assert np.allclose(sim.nout.t_written, out["t"], rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_run_parity_tight_tolerance(form):
+    """With the integrator error controlled (reltol 1e-8) the fused FP32 form follows
+    the FP64 oracle to rel-L2 <= 1e-4 in displacement after the first few centuries
+    (<= 2e-4 at t = 250 yr, where u is still small); the plain FP64 form to 1e-5."""
+    tout = np.arange(250.0, 2001.0, 250.0)
+    sim = small_sim(form, 32, 32, t_end=2000.0)
+    sim.cfg.reltol, sim.cfg.abstol = 1e-8, 1e-10
+    sim.nout.t = list(tout)
+    ref = pair(sim)
+    F.run(sim)
+    out = ref.run(tout, want=("u",))
+    for k in range(len(tout)):
+        e = rel_l2(F_(sim.nout.out["u"][k]), out["u"][k])
+        bound = 1e-5 if form == "fp64" else (1e-4 if tout[k] >= 500 else 2e-4)
+        assert e < bound, (form, tout[k], e)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_run_config1(form):
+    """Config 1 (N=64, 3000 km, Gaussian viscosity bump, 10 kyr, outputs every kyr)."""
+    sim = W.config1(form=form)
+    ref = pair(sim)
+    F.run(sim)
+    out = ref.run(np.asarray(sim.nout.t))
+    for k in range(len(sim.nout.t)):
+        e = rel_l2(F_(sim.nout.out["u"][k]), out["u"][k])
+        assert e < RUN_TOL[form], (form, k, "u", e)
+        e = rel_l2(F_(sim.nout.out["ue"][k]), out["ue"][k])
+        assert e < RUN_TOL_SPARSE[form], (form, k, "ue", e)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_coupling_steps_external_ice(form):
+    """init_integrator + step!(integrator, dt, true) with an externally updated load
+    (docs/src/examples/coupling.jl:22-34)."""
+    sim = small_sim(form, 32, 32, t_end=500.0, external=True)
+    sim.nout.t = [100.0, 300.0]
+    ref = pair(sim)
+    integ = F.init_integrator(sim)
+    ref.init_integrator(np.asarray(sim.nout.t))
+    H1 = 1e3 * (sim.domain.R < 0.4 * sim.domain.Wx)
+    tt = 0.0
+    for _ in range(5):
+        H = H1 * (1 - np.exp(-tt / 200.0))
+        sim.set_field("H_ice", H)
+        ref.set_field(abi.FIELDS["H_ice"], F_(H))
+        F.step(integ, 50.0, True)
+        ref.step(50.0)
+        tt += 50.0
+        e = rel_l2(F_(sim.get_field("u")), ref.get_field(abi.FIELDS["u"]))
+        assert e < RUN_TOL[form], (tt, e)
+    assert abs(integ.t - 250.0) < 1e-9
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_checkpoint_restore_bitwise(form):
+    sim = small_sim(form, 32, 32, t_end=600.0, external=True)
+    sim.set_field  # noqa
+    integ = F.init_integrator(sim)
+    H1 = 1e3 * (sim.domain.R < 0.4 * sim.domain.Wx)
+    sim.set_field("H_ice", H1)
+    F.step(integ, 100.0, True)
+    import ctypes as C
+    size = C.c_size_t(0)
+    lib = sim.lib
+    assert lib.fi_checkpoint(sim._handle, None, C.byref(size)) == 0
+    buf = (C.c_char * size.value)()
+    assert lib.fi_checkpoint(sim._handle, buf, C.byref(size)) == 0
+    F.step(integ, 200.0, True)
+    u_a = sim.get_field("u")
+    assert lib.fi_restore(sim._handle, buf, size) == 0
+    F.step(integ, 200.0, True)
+    u_b = sim.get_field("u")
+    assert np.array_equal(u_a, u_b)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_determinism(form):
+    outs = []
+    for _ in range(2):
+        sim = small_sim(form, 32, 32, t_end=500.0)
+        sim.nout.t = [500.0]
+        F.run(sim)
+        outs.append(sim.nout.out["u"][0])
+        sim.close()
+    assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_forcing_out_of_range_is_an_error(form):
+    sim = small_sim(form, 16, 16, t_end=100.0)
+    sim.init_problem()
+    u, d = sim.domain.zeros(), sim.domain.zeros()
+    with pytest.raises(abi.FiError) as ei:
+        F.update_diagnostics(d, u, sim, 150.0)
+    assert ei.value.code == abi.FI_ERR_FORCING_RANGE
+    # the handle stays usable
+    F.update_diagnostics(d, u, sim, 50.0)

@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark of the LV-ELVA hot path: kyr simulated per second on the N=350 glacial
+cycle (6000 km domain, seeded random viscosity / lithosphere / ice fields, elastic,
+viscous and sea-surface convolutions on), fused FP32 form on one B200.
+
+One bench step = advancing the simulation by one kyr of the glacial cycle
+(consecutive segments; about 17k adaptive BS3 steps each).  `value` is kyr/s with all
+inputs resident on the device (CUDA-event time on the library's stream); `e2e` is the
+same metric through the public coupling API (init_integrator / step! with an
+externally supplied ice field copied from host memory every step and the displacement
+read back).  Also reported: the plain FP64 form (the comparison baseline), the
+dominant kernel against the HBM roofline, and the CPU oracle timed on the host cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+import __graft_entry__  # noqa: E402
+
+__graft_entry__.load_package()
+import fastiso_b200 as F  # noqa: E402
+import fastiso_b200.workloads as W  # noqa: E402
+
+METRIC = "kyr simulated/s at N=350 vs plain FP64 GPU @relL2<=1e-4; ensemble member-kyr/s"
+SEG_YR = 1000.0
+N350 = 350
+PEAKS_PATH = ROOT / "MEASURED_PEAKS.json"
+
+
+def hbm_peak():
+    try:
+        return float(json.loads(PEAKS_PATH.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def l2_flush(dev):
+    """Write 256 MiB (> 126 MB L2) between timed steps."""
+    import torch
+
+    buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")
+    buf.fill_(1.0)
+    torch.cuda.synchronize(dev)
+    del buf
+
+
+def counters(sim):
+    st = sim.stats()
+    return {k: st[k] for k in ("nf", "naccept", "nreject", "nsparse", "segments", "gpu_ms")}
+
+
+def launches_between(a, b):
+    """Kernels launched by the step loop: 3 per right-hand side (rows_fwd, cols,
+    rows_inv), 3 per sparse update, 1 segment-start per graph launch."""
+    return 3 * (b["nf"] - a["nf"]) + 3 * (b["nsparse"] - a["nsparse"]) + (b["segments"] - a["segments"])
+
+
+def bytes_per_launch(nx, ny):
+    """Algorithmic bytes of each fused kernel (stage-2 variants as timed): every input
+    read once, every output written once, halo re-reads and twiddles not counted."""
+    n = nx * ny
+    NH = nx // 2 + 1
+    spec = 8 * NH * ny  # complex64 half spectrum
+    Mx, My = F.nextfastfft(2 * nx - 1), F.nextfastfft(2 * ny - 1)
+    MH = Mx // 2 + 1
+    return {
+        # uprev f64, k1, D, K/(2eta), two ice snapshots, ue, dz in; S, sig_load, sig_geo out
+        "k_rows_fwd": 8 * n + 4 * n * 7 + spec + 8 * n,
+        "k_cols": 2 * spec + 4 * NH * ny,
+        "k_rows_inv": spec + 4 * n,
+        "k_conv_rows": 2 * 4 * n + 2 * 8 * MH * ny,
+        "k_conv_cols": 2 * (8 * MH * ny + 8 * MH * My + 8 * MH * (ny + 2)),
+        "k_conv_rows_inv": 2 * 8 * MH * (ny + 2) + 2 * 4 * n,
+    }
+
+
+def roofline(dev, ms_step, per_step_launch):
+    sim = W.config2(form="fp32", N=N350)
+    sim.cfg.device = dev
+    F.init_integrator(sim)
+    import ctypes as C
+
+    ms = (C.c_double * 6)()
+    rc = sim.lib.fi_time_kernels(sim._handle, 200, ms)
+    if rc:
+        raise RuntimeError(f"fi_time_kernels failed ({rc})")
+    names = ["k_rows_fwd", "k_cols", "k_rows_inv", "k_conv_rows", "k_conv_cols", "k_conv_rows_inv"]
+    t = dict(zip(names, list(ms)))
+    share = {k: t[k] * per_step_launch[k] for k in names}
+    top = max(share, key=share.get)
+    bpl = bytes_per_launch(N350, N350)
+    peak, kind = hbm_peak()
+    achieved = bpl[top] / (t[top] * 1e-3) / 1e9
+    traffic = None
+    tpath = ROOT / "profiles" / "roofline_traffic.json"
+    if tpath.exists():
+        traffic = json.loads(tpath.read_text()).get(top)
+    sim.close()
+    return {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak, "peak_kind": kind,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+            "bytes_per_launch": bpl[top], "ms_per_launch": round(t[top], 5),
+            "kernel_ms": {k: round(v, 5) for k, v in t.items()}}
+
+
+def cpu_oracle_sample(seconds_target=12.0, seg=5.0):
+    """The FP64 oracle on the host cores: config-2 segments of `seg` yr until about
+    `seconds_target` of CPU work; returns (kyr/s, cores, years)."""
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    sim = W.config2(form="fp64", N=N350)
+    ref = O.oracle_for(sim)
+    ref.init()
+    ref.init_integrator([])
+    yrs, t_used = 0.0, 0.0
+    while t_used < seconds_target:
+        t0 = time.perf_counter()
+        ref.step(seg)
+        t_used += time.perf_counter() - t0
+        yrs += seg
+    return yrs / 1e3 / t_used, cores, yrs
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU semantics (the FP64 oracle, OpenMP over the
+    host cores), same metric and config; rank 0 only."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    seg = 5.0
+    sim = W.config2(form="fp64", N=N350)
+    ref = O.oracle_for(sim)
+    ref.init()
+    ref.init_integrator([])
+    for _ in range(args.warmup):
+        ref.step(seg)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.step(seg)
+    el = time.perf_counter() - t0
+    v = args.steps * seg / 1e3 / el
+    line = {"metric": METRIC, "value": v, "unit": "kyr/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fields)",
+            "impl": "reference",
+            "config": {"workload": "config2 glacial cycle N=350, 6000 km, elastic+viscous+sea-surface",
+                       "step": f"{seg} yr of simulated time per step (bounded CPU sample)"},
+            "cpu_baseline": {"value": v, "unit": "kyr/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} x {seg} yr of config2 after {args.warmup} x {seg} yr warm-up"},
+            "e2e": {"value": v, "unit": "kyr/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, rank, world, dev):
+    import torch
+
+    # ---- headline: fused FP32 form, inputs resident ------------------------------
+    sim = W.config2(form="fp32", N=N350)
+    sim.cfg.device = dev
+    sim.cfg.max_steps = 20_000_000
+    integ = F.init_integrator(sim)
+    for _ in range(args.warmup):
+        F.step(integ, SEG_YR, True)
+    c0 = counters(sim)
+    step_ms = []
+    with ClockSampler(dev) as clk:
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+        for _ in range(args.steps):
+            l2_flush(dev)
+            F.step(integ, SEG_YR, True)
+            step_ms.append(sim.stats()["last_gpu_ms"])
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            torch.distributed.barrier()
+    c1 = counters(sim)
+    t_total = float(sum(step_ms))
+    if world > 1:
+        tt = torch.tensor([t_total], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_total = float(tt.item())
+    kyr = args.steps * SEG_YR / 1e3
+    value = world * kyr / (t_total / 1e3)
+    attempts = (c1["naccept"] + c1["nreject"]) - (c0["naccept"] + c0["nreject"])
+    launches = launches_between(c0, c1)
+    sim.close()
+    if rank != 0:
+        return
+    # ---- e2e: coupling API with host buffers -------------------------------------
+    e2e_sim = W.config2(form="fp32", N=N350)
+    dom = e2e_sim.domain
+    _, _, _, H_field = W.config2_fields(N350, 3e6)
+    bcs = F.BoundaryConditions(dom, ice_thickness=F.ExternallyUpdatedIceThickness())
+    esim = F.Simulation(dom, bcs, e2e_sim.sealevel, e2e_sim.solidearth, (0.0, 120e3), form="fp32", device=dev,
+                        max_steps=20_000_000)
+    e2e_sim.close()
+    einteg = F.init_integrator(esim)
+    H_host = np.ascontiguousarray(H_field)
+    tt = 0.0
+    for _ in range(args.warmup):
+        esim.set_field("H_ice", H_host * W.sawtooth(tt + SEG_YR / 2))
+        F.step(einteg, SEG_YR, True)
+        tt += SEG_YR
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        esim.set_field("H_ice", H_host * W.sawtooth(tt + SEG_YR / 2))
+        F.step(einteg, SEG_YR, True)
+        u_host = esim.get_field("u")
+        tt += SEG_YR
+    e2e_el = time.perf_counter() - t0
+    e2e_val = kyr / e2e_el
+    assert np.isfinite(u_host).all()
+    esim.close()
+    # ---- plain FP64 form on a short window of the same workload ------------------
+    psim = W.config2(form="fp64", N=N350)
+    psim.cfg.device = dev
+    psim.cfg.max_steps = 20_000_000
+    pinteg = F.init_integrator(psim)
+    F.step(pinteg, 20.0, True)
+    p0 = psim.stats()
+    F.step(pinteg, 20.0, True)
+    p1 = psim.stats()
+    plain_kyr_s = 0.020 / (p1["last_gpu_ms"] / 1e3)
+    plain_ms_per_bs3 = p1["last_gpu_ms"] / max(1, (p1["naccept"] + p1["nreject"]) - (p0["naccept"] + p0["nreject"]))
+    psim.close()
+    # ---- roofline of the dominant kernel ----------------------------------------
+    per_step = {"k_rows_fwd": 3, "k_cols": 3, "k_rows_inv": 3, "k_conv_rows": 0, "k_conv_cols": 0,
+                "k_conv_rows_inv": 0}
+    rhs_per_attempt = (c1["nf"] - c0["nf"]) / max(1, attempts)
+    sparse_per_attempt = (c1["nsparse"] - c0["nsparse"]) / max(1, attempts)
+    for k in ("k_rows_fwd", "k_cols", "k_rows_inv"):
+        per_step[k] = rhs_per_attempt
+    for k in ("k_conv_rows", "k_conv_cols", "k_conv_rows_inv"):
+        per_step[k] = sparse_per_attempt
+    roof = roofline(dev, t_total / args.steps, per_step)
+    # ---- CPU baseline (oracle) ---------------------------------------------------
+    cpu_v, cores, yrs = cpu_oracle_sample()
+    line = {
+        "metric": METRIC, "value": value, "unit": "kyr/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 state)",
+        "data": "synthetic (seeded Gaussian random fields)",
+        "config": {"workload": "config2 glacial cycle N=350 over 6000 km, 121 ice snapshots, "
+                               "elastic+viscous+sea-surface, BS3 reltol=Float64(1f-5)",
+                   "step": f"{SEG_YR:g} yr of simulated time (consecutive segments)",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "256 MiB written between timed steps; one member's working set (~15 MB) is "
+                         "L2-resident within a step"},
+        "bs3_steps_per_bench_step": attempts / args.steps,
+        "us_per_bs3_step": 1e3 * t_total / max(1, attempts),
+        "rhs_evals_per_s": (c1["nf"] - c0["nf"]) / (t_total / 1e3),
+        "plain_fp64": {"value": plain_kyr_s, "unit": "kyr/s", "ms_per_bs3_step": plain_ms_per_bs3,
+                       "sample": "20 yr after 20 yr warm-up"},
+        "speedup_vs_plain_fp64": value / world / plain_kyr_s,
+        "ensemble": None,
+        "e2e": {"value": e2e_val, "unit": "kyr/s", "h2d_bytes_per_step": 8 * N350 * N350,
+                "d2h_bytes_per_step": 8 * N350 * N350,
+                "path": "init_integrator + per step: set H_ice (host) -> step!(1 kyr) -> read u (host)"},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "cpu_baseline": {"value": cpu_v, "unit": "kyr/s", "cores": cores, "kind": "port",
+                         "sample": f"FP64 oracle (C, OpenMP), config2 N=350, {yrs:g} yr from t=0"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fused", choices=["fused", "reference"])
+    ap.add_argument("--profile", action="store_true",
+                    help="only a short fused N=350 segment (10 yr warm-up + 5 yr) for ncu captures")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.profile:
+        sim = W.config2(form="fp32", N=N350)
+        sim.cfg.device = local
+        integ = F.init_integrator(sim)
+        F.step(integ, 10.0, True)
+        F.step(integ, 5.0, True)
+        print(json.dumps({"profile_case": "config2 N=350 fp32, 15 yr", "stats": sim.stats()}))
+        return
+    try:
+        run_gpu(args, rank, world, local)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

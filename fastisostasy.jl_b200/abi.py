@@ -104,7 +104,7 @@ class FiConfig(C.Structure):
         ("dt_sparse_diagnostics", C.c_double),
         ("max_steps", C.c_int64),
         ("form", C.c_int32),
-        ("reserved", C.c_int32),
+        ("device", C.c_int32),
     ]
 
 
@@ -120,6 +120,9 @@ class FiStats(C.Structure):
         ("nsparse", C.c_int64),
         ("status", C.c_int32),
         ("form", C.c_int32),
+        ("gpu_ms", C.c_double),
+        ("last_gpu_ms", C.c_double),
+        ("segments", C.c_int64),
     ]
 
 
@@ -154,7 +157,7 @@ def default_config(nx: int, ny: int, Wx: float, Wy: float) -> FiConfig:
     c.dt_sparse_diagnostics = 10.0
     c.max_steps = 1_000_000
     c.form = FI_FORM_FP32
-    c.reserved = 0
+    c.device = 0
     return c
 
 
@@ -198,6 +201,7 @@ _SIGS = {
     "fi_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FiStats)]),
     "fi_checkpoint": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]),
     "fi_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "fi_time_kernels": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "fi_last_error": (C.c_char_p, [C.c_void_p]),
     "fi_status_string": (C.c_char_p, [C.c_int32]),
     "fi_destroy": (None, [C.c_void_p]),

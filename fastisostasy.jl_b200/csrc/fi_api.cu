@@ -6,6 +6,7 @@
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -92,6 +93,9 @@ struct fi_handle {
     bool initialized = false, integ_started = false;
     int last_call = 0;  // 0: step loop, 1: fi_rhs
     bool fsal_pending = false;  // FSAL re-evaluation owed by the last output callback
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double gpu_ms = 0.0, last_gpu_ms = 0.0;
+    long long segments = 0;
     double last_rhs_t = 0.0;
     long long nf_plain = 0;
 };
@@ -247,6 +251,7 @@ int fi_create(const fi_config* cfg, fi_handle** out) {
     if (cfg->nx < 4 || cfg->ny < 4 || cfg->nx > 2048 || cfg->ny > 2048) return FI_ERR_ARG;
     if (!(cfg->Wx > 0) || !(cfg->Wy > 0) || !(cfg->t1 >= cfg->t0)) return FI_ERR_ARG;
     if (cfg->form != FI_FORM_FP32 && cfg->form != FI_FORM_FP64) return FI_ERR_ARG;
+    if (cudaSetDevice(cfg->device) != cudaSuccess) return FI_ERR_CUDA;
     fi_handle* h = new fi_handle();
     h->cfg = *cfg;
     h->nx = cfg->nx; h->ny = cfg->ny;
@@ -275,7 +280,10 @@ int fi_create(const fi_config* cfg, fi_handle** out) {
         delete h;
         return FI_ERR_CUDA;
     }
+    const char* ng = getenv("FI_NO_GRAPH");
+    if (ng && ng[0] == '1') h->graph_ok = false;  // host-driven step loop (profiling / debugging)
     int rc = create_buffers(h);
+    if (!rc && (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)) rc = FI_ERR_CUDA;
     if (rc) {
         fprintf(stderr, "fi_create: %s\n", h->err.c_str());
         fi_destroy(h);
@@ -287,7 +295,10 @@ int fi_create(const fi_config* cfg, fi_handle** out) {
 
 void fi_destroy(fi_handle* h) {
     if (!h) return;
+    cudaSetDevice(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->seg_exec) cudaGraphExecDestroy(h->seg_exec);
     if (h->seg_graph) cudaGraphDestroy(h->seg_graph);
     for (void* p : h->allocs) cudaFree(p);
@@ -513,6 +524,7 @@ static double haf_host(double rho_sw_ice, double H, double zb, double zss) {
 }
 
 extern "C" int fi_set_field(fi_handle* h, int32_t field, const double* host, size_t n) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || !host) return FI_ERR_ARG;
     if (n != N2(h)) return set_err(h, FI_ERR_ARG, "field size %zu != nx*ny", n);
     std::vector<double> v(host, host + n);
@@ -545,6 +557,7 @@ extern "C" int fi_set_field(fi_handle* h, int32_t field, const double* host, siz
 }
 
 extern "C" int fi_set_ice_history(fi_handle* h, int32_t K, const double* t, const double* H) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || K < 1 || !t || !H) return FI_ERR_ARG;
     for (int k = 1; k < K; k++)
         if (!(t[k] > t[k - 1])) return set_err(h, FI_ERR_ARG, "ice times must increase");
@@ -554,6 +567,7 @@ extern "C" int fi_set_ice_history(fi_handle* h, int32_t K, const double* t, cons
 }
 
 extern "C" int fi_set_elastic_table(fi_handle* h, int32_t n, const double* rm, const double* GE) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || n < 2 || !rm || !GE) return FI_ERR_ARG;
     h->rm.assign(rm, rm + n);
     h->GE.assign(GE, GE + n);
@@ -561,6 +575,7 @@ extern "C" int fi_set_elastic_table(fi_handle* h, int32_t n, const double* rm, c
 }
 
 extern "C" int fi_set_channel_scaling(fi_handle* h, int32_t n, const double* ratio, const double* thick) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || n < 0 || (n > 0 && (!ratio || !thick))) return FI_ERR_ARG;
     h->ch_ratio.assign(ratio, ratio + n);
     h->ch_thick.assign(thick, thick + n);
@@ -588,6 +603,7 @@ static int rhs_fused(fi_handle* h, int stage, const double* uin, float* vout, do
 static int rhs_plain(fi_handle* h, double t, double* u, double* dudt);
 
 extern "C" int fi_init(fi_handle* h) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h) return FI_ERR_ARG;
     if (h->initialized) return set_err(h, FI_ERR_STATE, "fi_init called twice");
     const fi_config& c = h->cfg;
@@ -786,6 +802,7 @@ static int rhs_fused(fi_handle* h, int stage, const double* uin, float* vout, do
 }
 
 extern "C" int fi_rhs(fi_handle* h, double t, double* u_inout, double* dudt_out) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || !u_inout || !dudt_out) return FI_ERR_ARG;
     if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
     const size_t n = N2(h);
@@ -1276,7 +1293,22 @@ static int record_output(fi_handle* h, int k, const OutBufs& o) {
 }
 
 // solve!(integrator): segments between tstops; outputs by nout_condition
+static int solve_until_(fi_handle* h, const OutBufs* o);
+
+// device time of one integration call, CUDA events on the handle's stream
 static int solve_until(fi_handle* h, const OutBufs* o) {
+    CK(cudaEventRecord(h->ev0, h->stream));
+    const int rc = solve_until_(h, o);
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->last_gpu_ms = ms;
+    h->gpu_ms += ms;
+    return rc;
+}
+
+static int solve_until_(fi_handle* h, const OutBufs* o) {
     const bool fused = h->cfg.form == FI_FORM_FP32;
     while (!h->tstops.empty()) {
         if (h->fsal_pending) {
@@ -1289,6 +1321,7 @@ static int solve_until(fi_handle* h, const OutBufs* o) {
         h->ctl.t_stop = h->tstops.front();
         if (fused) RET(write_ctl(h));
         if (fused) RET(run_segment_fused(h)); else RET(run_segment_plain(h));
+        h->segments += 1;
         Ctl& ct = h->ctl;
         if (ct.status != FI_OK)
             return set_err(h, ct.status, "integration stopped at t=%.6g: %s", ct.t, fi_status_string(ct.status));
@@ -1326,6 +1359,7 @@ static int set_tstops(fi_handle* h, int n, const double* ts, bool outputs) {
 
 extern "C" int fi_run(fi_handle* h, int32_t n_out, const double* t_out, double* out_t, double* out_u,
                       double* out_ue, double* out_dudt, double* out_dz_ss) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || n_out < 0 || (n_out > 0 && !t_out)) return FI_ERR_ARG;
     if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
     for (int k = 1; k < n_out; k++)
@@ -1341,6 +1375,7 @@ extern "C" int fi_run(fi_handle* h, int32_t n_out, const double* t_out, double* 
 }
 
 extern "C" int fi_init_integrator(fi_handle* h, int32_t n_tstops, const double* tstops) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || n_tstops < 0) return FI_ERR_ARG;
     if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
     RET(integ_start(h));
@@ -1353,6 +1388,7 @@ extern "C" int fi_init_integrator(fi_handle* h, int32_t n_tstops, const double* 
 }
 
 extern "C" int fi_step(fi_handle* h, double dt) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || !(dt > 0)) return FI_ERR_ARG;
     if (!h->integ_started) return set_err(h, FI_ERR_STATE, "fi_init_integrator not called");
     if (h->cfg.form == FI_FORM_FP32) RET(read_ctl(h));
@@ -1371,6 +1407,7 @@ extern "C" int fi_step(fi_handle* h, double dt) {
 }
 
 extern "C" int fi_get_stats(fi_handle* h, fi_stats* st) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || !st) return FI_ERR_ARG;
     memset(st, 0, sizeof(*st));
     if (h->initialized) RET(read_ctl(h));
@@ -1383,10 +1420,64 @@ extern "C" int fi_get_stats(fi_handle* h, fi_stats* st) {
     st->nsparse = ct.count_sparse;
     st->status = ct.status;
     st->form = h->cfg.form;
+    st->gpu_ms = h->gpu_ms;
+    st->last_gpu_ms = h->last_gpu_ms;
+    st->segments = h->segments;
+    return FI_OK;
+}
+
+extern "C" int fi_time_kernels(fi_handle* h, int32_t reps, double* ms) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h || !ms || reps < 1) return FI_ERR_ARG;
+    if (h->cfg.form != FI_FORM_FP32) return set_err(h, FI_ERR_UNSUPPORTED, "kernel timing is for the FP32 form");
+    if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
+    RET(read_ctl(h));
+    h->ctl.active = 1;
+    h->ctl.gate = 1;
+    h->ctl.status = FI_OK;
+    RET(write_ctl(h));
+    for (int k = 0; k < 6; k++) {
+        for (int r = -3; r < reps; r++) {
+            if (r == 0) CK(cudaEventRecord(h->ev0, h->stream));
+            switch (k) {
+                case 0:
+                    k_rows_fwd<<<h->n_rows, NT, rows_fwd_smem(h->nx, h->h_rows), h->stream>>>(
+                        h->d_mem, h->t_rows, h->d_plans, 2, h->h_rows, nullptr);
+                    break;
+                case 1:
+                    k_cols<<<h->n_cols, NT, cols_smem(h->ny, h->B_cols), h->stream>>>(h->d_mem, h->t_cols,
+                                                                                    h->d_plans, h->B_cols);
+                    break;
+                case 2:
+                    k_rows_inv<<<h->n_rows, NT, rows_inv_smem(h->nx, h->h_rows), h->stream>>>(
+                        h->d_mem, h->t_rows, h->d_plans, 2, h->h_rows, nullptr, nullptr, 0, 0);
+                    break;
+                case 3:
+                    k_conv_rows<<<h->n_crow, NT, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(
+                        h->d_mem, h->t_crow, h->d_plans, h->h_conv);
+                    break;
+                case 4:
+                    k_conv_cols<<<h->n_ccol, NT, conv_cols_smem(h->My, h->B_conv), h->stream>>>(
+                        h->d_mem, h->t_ccol, h->d_plans, h->B_conv);
+                    break;
+                default:
+                    k_conv_rows_inv<<<h->n_crowi, NT, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(
+                        h->d_mem, h->t_crowi, h->d_plans, h->h_conv);
+                    break;
+            }
+            CKL();
+        }
+        CK(cudaEventRecord(h->ev1, h->stream));
+        CK(cudaEventSynchronize(h->ev1));
+        float t = 0.0f;
+        CK(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+        ms[k] = (double)t / reps;
+    }
     return FI_OK;
 }
 
 extern "C" int fi_get_field(fi_handle* h, int32_t field, double* host, size_t n) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || !host) return FI_ERR_ARG;
     if (n != N2(h)) return set_err(h, FI_ERR_ARG, "field size %zu != nx*ny", n);
     std::vector<double> v;
@@ -1511,6 +1602,7 @@ static std::vector<Blob> state_blobs(fi_handle* h) {
 }
 
 extern "C" int fi_checkpoint(fi_handle* h, void* buf, size_t* size) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || !size) return FI_ERR_ARG;
     if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
     auto blobs = state_blobs(h);
@@ -1537,6 +1629,7 @@ extern "C" int fi_checkpoint(fi_handle* h, void* buf, size_t* size) {
 }
 
 extern "C" int fi_restore(fi_handle* h, const void* buf, size_t size) {
+    if (h) cudaSetDevice(h->cfg.device);
     if (!h || !buf) return FI_ERR_ARG;
     if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init must precede fi_restore");
     const char* r = (const char*)buf;

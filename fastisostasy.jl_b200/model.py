@@ -375,7 +375,7 @@ class Simulation:
     the default) or "fp64" (the plain FP64 form)."""
 
     def __init__(self, domain, bcs, sealevel, solidearth, t_span, *, opts=None, u_ref=None, ue_ref=None,
-                 dz_ss_ref=None, z_b_ref=None, nout=None, c=None, form="fp32", max_steps=1_000_000):
+                 dz_ss_ref=None, z_b_ref=None, nout=None, c=None, form="fp32", max_steps=1_000_000, device=0):
         self.domain, self.bcs, self.sealevel, self.solidearth = domain, bcs, sealevel, solidearth
         self.opts = opts or SolverOptions()
         self.c = c or PhysicalConstants()
@@ -425,6 +425,7 @@ class Simulation:
         cfg.dt_sparse_diagnostics = float(self.opts.dt_sparse_diagnostics)
         cfg.max_steps = int(max_steps)
         cfg.form = {"fp32": abi.FI_FORM_FP32, "fp64": abi.FI_FORM_FP64}[form]
+        cfg.device = int(device)
         self.form = form
         self.cfg = cfg
         self.elastic_table = get_greenintegrand_coeffs()

@@ -89,7 +89,7 @@ typedef struct fi_config {
     double dt_sparse_diagnostics;   /* 10 yr */
     int64_t max_steps;              /* step-attempt budget per run/step call (0 = unlimited) */
     int32_t form;                   /* FI_FORM_* */
-    int32_t reserved;
+    int32_t device;                 /* CUDA device ordinal the handle runs on */
 } fi_config;
 
 /* Fields addressable by fi_set_field / fi_get_field.  All are nx*ny doubles. */
@@ -128,6 +128,10 @@ typedef struct fi_stats {
     int64_t nsparse;          /* sparse elastic / sea-surface updates (count_sparse_updates) */
     int32_t status;           /* FI_OK or the device status code */
     int32_t form;
+    double gpu_ms;            /* device time of integration calls so far (CUDA events on
+                                 the handle's stream), ms */
+    double last_gpu_ms;       /* device time of the last fi_run / fi_step call, ms */
+    int64_t segments;         /* step-loop launches (one CUDA graph launch each) */
 } fi_stats;
 
 typedef struct fi_handle fi_handle;
@@ -189,6 +193,13 @@ int fi_get_stats(fi_handle* h, fi_stats* st);
  * buf == NULL writes the needed size into *size. */
 int fi_checkpoint(fi_handle* h, void* buf, size_t* size);
 int fi_restore(fi_handle* h, const void* buf, size_t size);
+
+/* Diagnostics (no counterpart in the reference): times each fused FP32 kernel with
+ * CUDA events over `reps` back-to-back launches on the handle's stream and writes the
+ * mean ms per launch of k_rows_fwd (stage 2), k_cols, k_rows_inv (stage 2),
+ * k_conv_rows, k_conv_cols and k_conv_rows_inv into ms[0..5].  It overwrites the
+ * handle's state; use a separate handle. */
+int fi_time_kernels(fi_handle* h, int32_t reps, double* ms);
 
 const char* fi_last_error(const fi_handle* h);
 const char* fi_status_string(int32_t status);

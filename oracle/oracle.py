@@ -201,3 +201,22 @@ def bs3_decay(lam, u0, t1, t_out, reltol=1e-3, abstol=1e-6):
     if rc:
         raise RuntimeError(f"bs3_decay failed {rc}")
     return u, ns.value
+
+
+def oracle_for(sim):
+    """An OracleSim fed the same host inputs as a library Simulation (fields, ice
+    history, Farrell table, channel scaling)."""
+    from fastiso_b200 import abi
+
+    inp = sim.prepared_inputs()
+    ref = OracleSim(inp["cfg"])
+    for name, arr in inp["fields"].items():
+        ref.set_field(abi.FIELDS[name], np.asarray(arr, dtype=np.float64).ravel(order="F"))
+    if inp["ice_t"] is not None:
+        ref.set_ice_history(inp["ice_t"], np.stack([np.asarray(h, dtype=np.float64).ravel(order="F")
+                                                    for h in inp["ice_H"]]))
+    ref.set_elastic_table(*inp["elastic_table"])
+    ratio, thick = inp["channels"]
+    if ratio.size:
+        ref.set_channel_scaling(ratio, thick)
+    return ref

@@ -14,18 +14,7 @@ def F_(a):
     return np.asarray(a, dtype=np.float64).ravel(order="F")
 
 
-def oracle_for(sim: F.Simulation) -> O.OracleSim:
-    inp = sim.prepared_inputs()
-    ref = O.OracleSim(inp["cfg"])
-    for name, arr in inp["fields"].items():
-        ref.set_field(abi.FIELDS[name], F_(arr))
-    if inp["ice_t"] is not None:
-        ref.set_ice_history(inp["ice_t"], np.stack([F_(h) for h in inp["ice_H"]]))
-    ref.set_elastic_table(*inp["elastic_table"])
-    ratio, thick = inp["channels"]
-    if ratio.size:
-        ref.set_channel_scaling(ratio, thick)
-    return ref
+oracle_for = O.oracle_for
 
 
 def rel_l2(a, b):

@@ -32,6 +32,7 @@ struct Plan {
     int L;
     int npass;
     int radix[FFT_MAX_PASSES];
+    unsigned mag_nb[FFT_MAX_PASSES], mag_ns[FFT_MAX_PASSES];
     float2* tw32;
     double2* tw64;
 };
@@ -96,6 +97,7 @@ struct fi_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double gpu_ms = 0.0, last_gpu_ms = 0.0;
     long long segments = 0;
+    size_t smem_cap = 0;
     double last_rhs_t = 0.0;
     long long nf_plain = 0;
 };
@@ -155,6 +157,11 @@ static int get_plan(fi_handle* h, int L, int* out) {
     for (int f = 11; f * f <= m; f += 2) while (m % f == 0) { p.radix[np++] = f; m /= f; }
     if (m > 1) p.radix[np++] = m;
     p.npass = np;
+    for (int i = 0, Ns = 1; i < np; i++) {
+        p.mag_nb[i] = fastdiv_magic((unsigned)(L / p.radix[i]));
+        p.mag_ns[i] = fastdiv_magic((unsigned)Ns);
+        Ns *= p.radix[i];
+    }
     std::vector<double2> t64(L);
     std::vector<float2> t32(L);
     for (int k = 0; k < L; k++) {
@@ -179,6 +186,8 @@ static int upload_plans(fi_handle* h) {
         v[i].L = h->plans[i].L;
         v[i].npass = h->plans[i].npass;
         memcpy(v[i].radix, h->plans[i].radix, sizeof(v[i].radix));
+        memcpy(v[i].mag_nb, h->plans[i].mag_nb, sizeof(v[i].mag_nb));
+        memcpy(v[i].mag_ns, h->plans[i].mag_ns, sizeof(v[i].mag_ns));
         v[i].tw32 = h->plans[i].tw32;
         v[i].tw64 = h->plans[i].tw64;
     }
@@ -333,6 +342,20 @@ static int create_buffers(fi_handle* h) {
         m.Mx = h->Mx; m.My = h->My; m.MH = h->MH; m.msp = h->msp;
         m.i1 = h->i1; m.j1 = h->j1;
         m.plan_x = h->plan_x; m.plan_y = h->plan_y; m.plan_Mx = h->plan_Mx; m.plan_My = h->plan_My;
+        auto cp = [&](FftPlan& dst, int idx) {
+            const Plan& q = h->plans[idx];
+            dst.L = q.L;
+            dst.npass = q.npass;
+            memcpy(dst.radix, q.radix, sizeof(dst.radix));
+            memcpy(dst.mag_nb, q.mag_nb, sizeof(dst.mag_nb));
+            memcpy(dst.mag_ns, q.mag_ns, sizeof(dst.mag_ns));
+            dst.tw32 = q.tw32;
+            dst.tw64 = q.tw64;
+        };
+        cp(m.px, h->plan_x);
+        cp(m.py, h->plan_y);
+        cp(m.pMx, h->plan_Mx);
+        cp(m.pMy, h->plan_My);
         for (int b = 0; b < 2; b++) {
             RET(dalloc(h, &m.u[b], n));
             RET(dalloc(h, &m.k14[b], n));
@@ -392,18 +415,14 @@ static int create_buffers(fi_handle* h) {
         RET(mk(&h->t_crow, h->n_crow));
         RET(mk(&h->t_ccol, h->n_ccol));
         RET(mk(&h->t_crowi, h->n_crowi));
-        const size_t smax = 227 * 1024;
-        const size_t s1 = rows_fwd_smem(h->nx, h->h_rows), s2 = cols_smem(h->ny, h->B_cols),
-                     s3 = rows_inv_smem(h->nx, h->h_rows), s4 = conv_rows_smem(h->Mx, h->h_conv),
-                     s5 = conv_cols_smem(h->My, h->B_conv);
-        if (s1 > smax || s2 > smax || s3 > smax || s4 > smax || s5 > smax)
-            return set_err(h, FI_ERR_ARG, "shared memory need exceeds 227 KB");
-        CK(cudaFuncSetAttribute(k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
-        CK(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s2));
-        CK(cudaFuncSetAttribute(k_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s3));
-        CK(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4));
-        CK(cudaFuncSetAttribute(k_conv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s5));
-        CK(cudaFuncSetAttribute(k_conv_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s4));
+        // opt in to the full shared memory per block; the actual need (which depends on the
+        // ice-table length) is checked in fi_init
+        int smax = 0;
+        CK(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->cfg.device));
+        const void* fk[] = {(const void*)k_rows_fwd, (const void*)k_cols, (const void*)k_rows_inv,
+                            (const void*)k_conv_rows, (const void*)k_conv_cols, (const void*)k_conv_rows_inv};
+        for (const void* f : fk) CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smax - 4096));
+        h->smem_cap = (size_t)(smax - 4096);
     } else {
         PlainBufs& p = h->p;
         const size_t M = (size_t)h->Mx * h->My;
@@ -670,6 +689,13 @@ extern "C" int fi_init(fi_handle* h) {
     ct.active = 1;
     ct.t_stop = c.t1;
     if (c.form == FI_FORM_FP32) {
+        const int K = (int)h->ice_t.size();
+        const size_t need[] = {rows_fwd_smem(h->nx, h->h_rows, 1, K), cols_smem(h->ny, h->B_cols),
+                               rows_inv_smem(h->nx, h->h_rows), conv_rows_smem(h->Mx, h->h_conv),
+                               conv_cols_smem(h->My, h->B_conv)};
+        for (size_t q : need)
+            if (q + sizeof(fi::Member) + sizeof(fi::Ctl) + 4096 > h->smem_cap)
+                return set_err(h, FI_ERR_ARG, "shared memory need %zu B exceeds the per-block limit", q);
         Member& m = h->mem;
         m.dx = h->dx; m.dy = h->dy; m.A = h->dx * h->dy;
         m.g = c.g; m.rho_ice = c.rho_ice; m.rho_litho = c.rho_litho; m.rho_um = c.rho_uppermantle;
@@ -768,28 +794,35 @@ extern "C" int fi_init(fi_handle* h) {
 // stage 1: state -> k1 slot), t taken from ctl.t_call
 // ---------------------------------------------------------------------------
 static int launch_sparse(fi_handle* h) {
-    k_conv_rows<<<h->n_crow, NT, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(h->d_mem, h->t_crow, h->d_plans,
-                                                                              h->h_conv);
+    k_conv_rows<<<h->n_crow, ROW_THREADS, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(h->d_mem, h->t_crow,
+                                                                                       h->h_conv);
     CKL();
-    k_conv_cols<<<h->n_ccol, NT, conv_cols_smem(h->My, h->B_conv), h->stream>>>(h->d_mem, h->t_ccol, h->d_plans,
-                                                                              h->B_conv);
+    k_conv_cols<<<h->n_ccol, ROW_THREADS, conv_cols_smem(h->My, h->B_conv), h->stream>>>(h->d_mem, h->t_ccol,
+                                                                                       h->B_conv);
     CKL();
-    k_conv_rows_inv<<<h->n_crowi, NT, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(h->d_mem, h->t_crowi,
-                                                                                   h->d_plans, h->h_conv);
+    k_conv_rows_inv<<<h->n_crowi, ROW_THREADS, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(
+        h->d_mem, h->t_crowi, h->h_conv);
     CKL();
     return FI_OK;
 }
 
+// One host-driven right-hand side body (stage 0/1) or one graph-free BS3 stage
+// (stages 2-4, fallback loop): forward rows, columns, and for stages 0/1/4 the
+// inverse rows.
 static int launch_rhs_body(fi_handle* h, int stage, const double* uin, float* vout, double* cout,
                            cudaGraphConditionalHandle hg, cudaGraphConditionalHandle hw) {
-    k_rows_fwd<<<h->n_rows, NT, rows_fwd_smem(h->nx, h->h_rows), h->stream>>>(h->d_mem, h->t_rows, h->d_plans,
-                                                                             stage, h->h_rows, uin);
+    const int inv = (stage == 3 || stage == 4) ? 1 : 0;
+    k_rows_fwd<<<h->n_rows, ROW_THREADS, rows_fwd_smem(h->nx, h->h_rows, inv, (int)h->ice_t.size()), h->stream>>>(
+        h->d_mem, h->t_rows, stage, h->h_rows, uin, inv);
     CKL();
-    k_cols<<<h->n_cols, NT, cols_smem(h->ny, h->B_cols), h->stream>>>(h->d_mem, h->t_cols, h->d_plans, h->B_cols);
+    const int next = (stage == 2 || stage == 3) ? stage + 1 : 0;
+    k_cols<<<h->n_cols, ROW_THREADS, cols_smem(h->ny, h->B_cols), h->stream>>>(h->d_mem, h->t_cols, h->B_cols, next, 0);
     CKL();
-    k_rows_inv<<<h->n_rows, NT, rows_inv_smem(h->nx, h->h_rows), h->stream>>>(h->d_mem, h->t_rows, h->d_plans,
-                                                                            stage, h->h_rows, vout, cout, hg, hw);
-    CKL();
+    if (stage <= 1 || stage == 4) {
+        k_rows_inv<<<h->n_rows, ROW_THREADS, rows_inv_smem(h->nx, h->h_rows), h->stream>>>(
+            h->d_mem, h->t_rows, stage, h->h_rows, vout, cout, hg, hw);
+        CKL();
+    }
     return FI_OK;
 }
 
@@ -1073,7 +1106,7 @@ static int add_kernel(fi_handle* h, cudaGraph_t g, cudaGraphNode_t* prev, void* 
     cudaKernelNodeParams kp{};
     kp.func = func;
     kp.gridDim = dim3(grid);
-    kp.blockDim = dim3(NT);
+    kp.blockDim = dim3(ROW_THREADS);
     kp.sharedMemBytes = (unsigned)smem;
     kp.kernelParams = args;
     cudaGraphNode_t node;
@@ -1099,14 +1132,13 @@ static int add_cond(fi_handle* h, cudaGraph_t g, cudaGraphNode_t* prev, cudaGrap
 static int add_sparse(fi_handle* h, cudaGraph_t g) {
     cudaGraphNode_t prev = nullptr;
     const Member* mp = h->d_mem;
-    const FftPlan* pp = h->d_plans;
     const Task *t1 = h->t_crow, *t2 = h->t_ccol, *t3 = h->t_crowi;
     int hc = h->h_conv, bc = h->B_conv;
-    void* a1[] = {(void*)&mp, (void*)&t1, (void*)&pp, (void*)&hc};
+    void* a1[] = {(void*)&mp, (void*)&t1, (void*)&hc};
     RET(add_kernel(h, g, &prev, (void*)k_conv_rows, h->n_crow, conv_rows_smem(h->Mx, hc), a1));
-    void* a2[] = {(void*)&mp, (void*)&t2, (void*)&pp, (void*)&bc};
+    void* a2[] = {(void*)&mp, (void*)&t2, (void*)&bc};
     RET(add_kernel(h, g, &prev, (void*)k_conv_cols, h->n_ccol, conv_cols_smem(h->My, bc), a2));
-    void* a3[] = {(void*)&mp, (void*)&t3, (void*)&pp, (void*)&hc};
+    void* a3[] = {(void*)&mp, (void*)&t3, (void*)&hc};
     RET(add_kernel(h, g, &prev, (void*)k_conv_rows_inv, h->n_crowi, conv_rows_smem(h->Mx, hc), a3));
     return FI_OK;
 }
@@ -1119,7 +1151,6 @@ static int build_segment_graph(fi_handle* h) {
     CK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
     for (int i = 0; i < 3; i++) CK(cudaGraphConditionalHandleCreate(&hg[i], g, 0, cudaGraphCondAssignDefault));
     const Member* mp = h->d_mem;
-    const FftPlan* pp = h->d_plans;
     int one = 1;
     cudaGraphNode_t prev = nullptr;
     {
@@ -1140,19 +1171,22 @@ static int build_segment_graph(fi_handle* h) {
         RET(add_sparse(h, sb));
         const Task* tr = h->t_rows;
         const Task* tc = h->t_cols;
-        int stage = s, hr = h->h_rows, bcol = h->B_cols;
+        int stage = s, hr = h->h_rows, bcol = h->B_cols, inv = (s > 2) ? 1 : 0;
+        int next = (s < 4) ? s + 1 : 0;
         const double* uin = nullptr;
         float* vout = nullptr;
         double* cout = nullptr;
-        cudaGraphConditionalHandle hnext = (s < 4) ? hg[s - 1] : hg[0];
-        cudaGraphConditionalHandle hloop = (s == 4) ? hw : 0;
-        void* a1[] = {(void*)&mp, (void*)&tr, (void*)&pp, (void*)&stage, (void*)&hr, (void*)&uin};
-        RET(add_kernel(h, body, &bp, (void*)k_rows_fwd, h->n_rows, rows_fwd_smem(h->nx, hr), a1));
-        void* a2[] = {(void*)&mp, (void*)&tc, (void*)&pp, (void*)&bcol};
+        cudaGraphConditionalHandle hnext = (s < 4) ? hg[s - 1] : 0;
+        void* a1[] = {(void*)&mp, (void*)&tr, (void*)&stage, (void*)&hr, (void*)&uin, (void*)&inv};
+        RET(add_kernel(h, body, &bp, (void*)k_rows_fwd, h->n_rows, rows_fwd_smem(h->nx, hr, inv, (int)h->ice_t.size()), a1));
+        void* a2[] = {(void*)&mp, (void*)&tc, (void*)&bcol, (void*)&next, (void*)&hnext};
         RET(add_kernel(h, body, &bp, (void*)k_cols, h->n_cols, cols_smem(h->ny, bcol), a2));
-        void* a3[] = {(void*)&mp, (void*)&tr, (void*)&pp, (void*)&stage, (void*)&hr,
-                      (void*)&vout, (void*)&cout, (void*)&hnext, (void*)&hloop};
-        RET(add_kernel(h, body, &bp, (void*)k_rows_inv, h->n_rows, rows_inv_smem(h->nx, hr), a3));
+        if (s == 4) {
+            cudaGraphConditionalHandle hgate = hg[0], hloop = hw;
+            void* a3[] = {(void*)&mp, (void*)&tr, (void*)&stage, (void*)&hr,
+                          (void*)&vout, (void*)&cout, (void*)&hgate, (void*)&hloop};
+            RET(add_kernel(h, body, &bp, (void*)k_rows_inv, h->n_rows, rows_inv_smem(h->nx, hr), a3));
+        }
     }
     CK(cudaGraphInstantiate(&h->seg_exec, g, 0));
     return FI_OK;
@@ -1441,28 +1475,28 @@ extern "C" int fi_time_kernels(fi_handle* h, int32_t reps, double* ms) {
             if (r == 0) CK(cudaEventRecord(h->ev0, h->stream));
             switch (k) {
                 case 0:
-                    k_rows_fwd<<<h->n_rows, NT, rows_fwd_smem(h->nx, h->h_rows), h->stream>>>(
-                        h->d_mem, h->t_rows, h->d_plans, 2, h->h_rows, nullptr);
+                    k_rows_fwd<<<h->n_rows, ROW_THREADS, rows_fwd_smem(h->nx, h->h_rows, 1, (int)h->ice_t.size()), h->stream>>>(
+                        h->d_mem, h->t_rows, 3, h->h_rows, nullptr, 1);
                     break;
                 case 1:
-                    k_cols<<<h->n_cols, NT, cols_smem(h->ny, h->B_cols), h->stream>>>(h->d_mem, h->t_cols,
-                                                                                    h->d_plans, h->B_cols);
+                    k_cols<<<h->n_cols, ROW_THREADS, cols_smem(h->ny, h->B_cols), h->stream>>>(
+                        h->d_mem, h->t_cols, h->B_cols, 0, 0);
                     break;
                 case 2:
-                    k_rows_inv<<<h->n_rows, NT, rows_inv_smem(h->nx, h->h_rows), h->stream>>>(
-                        h->d_mem, h->t_rows, h->d_plans, 2, h->h_rows, nullptr, nullptr, 0, 0);
+                    k_rows_inv<<<h->n_rows, ROW_THREADS, rows_inv_smem(h->nx, h->h_rows), h->stream>>>(
+                        h->d_mem, h->t_rows, 1, h->h_rows, nullptr, nullptr, 0, 0);
                     break;
                 case 3:
-                    k_conv_rows<<<h->n_crow, NT, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(
-                        h->d_mem, h->t_crow, h->d_plans, h->h_conv);
+                    k_conv_rows<<<h->n_crow, ROW_THREADS, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(
+                        h->d_mem, h->t_crow, h->h_conv);
                     break;
                 case 4:
-                    k_conv_cols<<<h->n_ccol, NT, conv_cols_smem(h->My, h->B_conv), h->stream>>>(
-                        h->d_mem, h->t_ccol, h->d_plans, h->B_conv);
+                    k_conv_cols<<<h->n_ccol, ROW_THREADS, conv_cols_smem(h->My, h->B_conv), h->stream>>>(
+                        h->d_mem, h->t_ccol, h->B_conv);
                     break;
                 default:
-                    k_conv_rows_inv<<<h->n_crowi, NT, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(
-                        h->d_mem, h->t_crowi, h->d_plans, h->h_conv);
+                    k_conv_rows_inv<<<h->n_crowi, ROW_THREADS, conv_rows_smem(h->Mx, h->h_conv), h->stream>>>(
+                        h->d_mem, h->t_crowi, h->h_conv);
                     break;
             }
             CKL();

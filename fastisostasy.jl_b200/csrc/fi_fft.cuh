@@ -31,13 +31,25 @@ constexpr int FFT_MAX_PASSES = 20;
 constexpr int FFT_MAX_LEN = 4096;
 
 // One transform length: radix schedule + twiddle tables tw[m] = exp(-2 pi i m / L).
+// mag_nb / mag_ns: multiply-high reciprocals of L/R and of Ns for each pass
+// (x / d == __umulhi(x, ceil(2^32 / d)) for x * d < 2^32; d == 1 is special-cased).
 struct FftPlan {
     int L;
     int npass;
     int radix[FFT_MAX_PASSES];
+    unsigned int mag_nb[FFT_MAX_PASSES];
+    unsigned int mag_ns[FFT_MAX_PASSES];
     const float2* tw32;
     const double2* tw64;
 };
+
+__host__ __device__ inline unsigned int fastdiv_magic(unsigned int d) {
+    return d <= 1 ? 0u : (unsigned int)((0x100000000ull + d - 1) / d);
+}
+
+__device__ __forceinline__ unsigned int fastdiv(unsigned int x, unsigned int d, unsigned int m) {
+    return d == 1 ? x : __umulhi(x, m);
+}
 
 template <typename T> __device__ __forceinline__ const cplx<T>* plan_tw(const FftPlan& p);
 template <> __device__ __forceinline__ const float2* plan_tw<float>(const FftPlan& p) { return p.tw32; }
@@ -164,30 +176,31 @@ template <bool INV, typename T> struct SmallDft<8, INV, T> {
 template <int R, bool INV, typename T>
 __device__ __forceinline__ void stockham_pass(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst,
                                               const cplx<T>* __restrict__ tw, int L, int Ns, int nbatch,
-                                              int bstride, int tid, int nth) {
+                                              int bstride, int tid, int nth, unsigned int mnb, unsigned int mns) {
     using C = cplx<T>;
     const int nb = L / R;
     const int stride = L / (Ns * R);
     const int total = nbatch * nb;
     for (int idx = tid; idx < total; idx += nth) {
-        const int b = idx / nb;
+        const int b = (int)fastdiv((unsigned)idx, (unsigned)nb, mnb);
         const int j = idx - b * nb;
         const C* s = src + b * bstride;
         C* d = dst + b * bstride;
-        const int k = j % Ns;
+        const int jq = (int)fastdiv((unsigned)j, (unsigned)Ns, mns);
+        const int k = j - jq * Ns;
         C v[R];
 #pragma unroll
         for (int r = 0; r < R; r++) v[r] = s[j + r * nb];
         if (Ns > 1) {
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                C w = __ldg(&tw[k * r * stride]);
+                C w = tw[k * r * stride];  // shared (FP32 kernels) or global (FP64)
                 if (INV) w.y = -w.y;
                 v[r] = cmul(v[r], w);
             }
         }
         SmallDft<R, INV, T>::run(v);
-        const int idxD = (j / Ns) * Ns * R + k;
+        const int idxD = jq * Ns * R + k;
 #pragma unroll
         for (int q = 0; q < R; q++) d[idxD + q * Ns] = v[q];
     }
@@ -214,7 +227,7 @@ __device__ __forceinline__ void stockham_pass_generic(const cplx<T>* __restrict_
             C v = s[j + r * nb];
             // twiddle w_L^(k r stride) then w_R^(q r) = w_L^((q r mod R) * nb)
             const int e = (k * r * stride + ((q * r) % R) * nb) % L;
-            C w = __ldg(&tw[e]);
+            C w = tw[e];
             if (INV) w.y = -w.y;
             acc = cadd(acc, cmul(v, w));
         }
@@ -235,13 +248,14 @@ __device__ cplx<T>* fft_batch(cplx<T>* buf0, cplx<T>* buf1, const FftPlan& p, in
     int Ns = 1;
     for (int ps = 0; ps < p.npass; ps++) {
         const int R = p.radix[ps];
+        const unsigned mnb = p.mag_nb[ps], mns = p.mag_ns[ps];
         switch (R) {
-            case 2: stockham_pass<2, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth); break;
-            case 3: stockham_pass<3, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth); break;
-            case 4: stockham_pass<4, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth); break;
-            case 5: stockham_pass<5, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth); break;
-            case 7: stockham_pass<7, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth); break;
-            case 8: stockham_pass<8, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth); break;
+            case 2: stockham_pass<2, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 3: stockham_pass<3, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 4: stockham_pass<4, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 5: stockham_pass<5, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 7: stockham_pass<7, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 8: stockham_pass<8, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
             default: stockham_pass_generic<INV, T>(src, dst, tw, p.L, R, Ns, nbatch, bstride, tid, nth); break;
         }
         __syncthreads();

@@ -64,6 +64,7 @@ struct Member {
     int Mx, My, MH, msp;        // convolution padded sizes, half width, pitch
     int i1, j1;                 // 0-based crop origin of samesize_conv
     int plan_x, plan_y, plan_Mx, plan_My;
+    FftPlan px, py, pMx, pMy;   // copies of the plans (kernels stage them in shared memory)
     int K;                      // ice snapshots
     int ice_external, ice_flat;
     int elastic_on, geoid_on, column_compressible;
@@ -119,5 +120,9 @@ struct Task {
     int member;
     int tile;
 };
+
+static_assert(sizeof(Member) % 8 == 0, "Member is copied as 8-byte words");
+static_assert(sizeof(Ctl) % 8 == 0, "Ctl is copied as 8-byte words");
+constexpr int TICE_MAX = 4096;  // ice-time tables up to this length are searched in shared memory
 
 }  // namespace fi

@@ -8,15 +8,13 @@ namespace fi {
 
 // ---- fused FP32 form (fi_fused.cu) ----
 __global__ void k_gate(const Member* mems, int nmem, double t, int use_ctl_t);
-__global__ void k_rows_fwd(const Member* mems, const Task* tasks, const FftPlan* plans, int stage, int h,
-                           const double* uin);
-__global__ void k_cols(const Member* mems, const Task* tasks, const FftPlan* plans, int B);
-__global__ void k_rows_inv(const Member* mems, const Task* tasks, const FftPlan* plans, int stage, int h,
-                           float* vout, double* cout, cudaGraphConditionalHandle h_gate,
-                           cudaGraphConditionalHandle h_loop);
-__global__ void k_conv_rows(const Member* mems, const Task* tasks, const FftPlan* plans, int h);
-__global__ void k_conv_cols(const Member* mems, const Task* tasks, const FftPlan* plans, int B);
-__global__ void k_conv_rows_inv(const Member* mems, const Task* tasks, const FftPlan* plans, int h);
+__global__ void k_rows_fwd(const Member* mems, const Task* tasks, int stage, int h, const double* uin, int inv_prev);
+__global__ void k_cols(const Member* mems, const Task* tasks, int B, int next_stage, cudaGraphConditionalHandle h_gate);
+__global__ void k_rows_inv(const Member* mems, const Task* tasks, int stage, int h, float* vout, double* cout,
+                           cudaGraphConditionalHandle h_gate, cudaGraphConditionalHandle h_loop);
+__global__ void k_conv_rows(const Member* mems, const Task* tasks, int h);
+__global__ void k_conv_cols(const Member* mems, const Task* tasks, int B);
+__global__ void k_conv_rows_inv(const Member* mems, const Task* tasks, int h);
 __global__ void k_segment_start(const Member* mems, int nmem, cudaGraphConditionalHandle h_gate,
                                 cudaGraphConditionalHandle h_loop);
 __global__ void kf_initdt_norms(const double* u, const float* v, const double* vc, double border, double abstol,
@@ -26,7 +24,8 @@ __global__ void kf_initdt_u1(double* u1, const double* u, const float* v, const 
 __global__ void kf_initdt_d2(const double* u, const float* v0, const double* c0p, const float* v1,
                              const double* c1p, double border, double abstol, double reltol, double* partial,
                              size_t n);
-size_t rows_fwd_smem(int nx, int h);
+size_t rows_fwd_smem(int nx, int h, int inv, int K);
+constexpr int ROW_THREADS = 512;
 size_t cols_smem(int ny, int B);
 size_t rows_inv_smem(int nx, int h);
 size_t conv_rows_smem(int Mx, int h);

@@ -193,6 +193,7 @@ _SIGS = {
     "fi_set_channel_scaling": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fi_init": (C.c_int, [C.c_void_p]),
     "fi_rhs": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fi_rhs_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
     "fi_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
                          C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                          C.POINTER(C.c_double)]),

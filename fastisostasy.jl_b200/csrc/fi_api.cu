@@ -17,6 +17,7 @@
 #include "../../include/fastiso_b200.h"
 #include "fi_device.cuh"
 #include "fi_kernels.h"
+#include "fi_noalloc.cuh"
 #include "fi_plain.h"
 
 using namespace fi;
@@ -863,6 +864,36 @@ extern "C" int fi_rhs(fi_handle* h, double t, double* u_inout, double* dudt_out)
         CK(cudaMemcpyAsync(dudt_out, h->p.fscratch, n * 8, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
+    h->last_call = 1;
+    h->last_rhs_t = t;
+    return FI_OK;
+}
+
+static_assert((size_t)FI_NOALLOC_MAX_CELLS == NOALLOC_MAX_CELLS, "scratch limit mismatch");
+
+// fi_rhs on device buffers with the result scratch in a static device array
+// (fi_noalloc.cu): no device or host allocation on the success path.
+extern "C" int fi_rhs_noalloc(fi_handle* h, double t, double* u_dev, double* dudt_dev) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h || !u_dev || !dudt_dev) return FI_ERR_ARG;
+    const size_t n = N2(h);
+    if (n > NOALLOC_MAX_CELLS)
+        return set_err(h, FI_ERR_ARG, "fi_rhs_noalloc: grid of %zu cells exceeds the static scratch limit of %zu cells",
+                       n, NOALLOC_MAX_CELLS);
+    if (h->cfg.form != FI_FORM_FP32) return set_err(h, FI_ERR_ARG, "fi_rhs_noalloc serves the FP32 form only");
+    if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
+    void* scr = nullptr;
+    CK(noalloc_scratch(&scr));
+    RET(read_ctl(h));
+    h->ctl.t_call = t;
+    h->ctl.status = FI_OK;
+    RET(write_ctl(h));
+    RET(rhs_fused(h, 0, u_dev, (float*)scr, (double*)((unsigned char*)scr + NOALLOC_CORNER_OFFSET)));
+    RET(read_ctl(h));
+    if (h->ctl.status) return set_err(h, h->ctl.status, "%s", fi_status_string(h->ctl.status));
+    CK(cudaMemcpyAsync(u_dev, h->mem.u[h->ctl.ibuf ^ 1], n * 8, cudaMemcpyDeviceToDevice, h->stream));
+    CK(noalloc_finish(scr, h->cfg.bc_viscous_border, n, dudt_dev, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     h->last_call = 1;
     h->last_rhs_t = t;
     return FI_OK;

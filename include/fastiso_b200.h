@@ -174,6 +174,24 @@ int fi_init(fi_handle* h);
  * viscous corner boundary condition exactly as in the reference. */
 int fi_rhs(fi_handle* h, double t, double* u_inout, double* dudt_out);
 
+/* No counterpart in the reference: fi_rhs for callers that may not allocate
+ * memory, e.g. a coupled ice-sheet model that keeps its state in device
+ * arrays and runs with device memory fully reserved by its own pool, or that
+ * cannot afford the device-wide synchronisation of cudaMalloc/cudaFree inside
+ * its time loop.  u_dev / dudt_dev are DEVICE pointers (nx*ny doubles, layout as
+ * for fi_set_field) on the handle's device; same results and side effects as
+ * fi_rhs.  FP32 form only.  On success the call allocates nothing, on the device
+ * or the host: its result scratch is a static device array of
+ * FI_NOALLOC_MAX_CELLS * 4 + 256 bytes (4 MiB) per device, and grids with more
+ * than FI_NOALLOC_MAX_CELLS cells are rejected with FI_ERR_ARG.  The first call
+ * on each device looks up the scratch address once (cudaGetSymbolAddress, that
+ * device current); make that first call before any stream capture starts.  All
+ * handles on a device share the scratch: calls that overlap in time on one
+ * device (from several host threads) race on it and must be serialised by the
+ * caller.  The call returns after its device work has finished. */
+#define FI_NOALLOC_MAX_CELLS (1024 * 1024)
+int fi_rhs_noalloc(fi_handle* h, double t, double* u_dev, double* dudt_dev);
+
 /* run!(sim) with NativeOutput times t_out (src/simulation.jl:236-262): integrates
  * t0 -> t1 with BS3 and the reference tolerances; at each output (same callback
  * semantics as nout_condition/nout_affect!) copies u, ue, dudt and dz_ss into

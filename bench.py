@@ -123,6 +123,30 @@ def launches_between(a, b):
     return 3 * (b["nf"] - a["nf"]) + 3 * (b["nsparse"] - a["nsparse"]) + (b["segments"] - a["segments"])
 
 
+def phase_timeline(sim, integ, years=50.0):
+    """Per-phase time of the persistent executor (block 0's view: the slowest block of
+    the phase plus the grid barrier), from fi_trace_phases over `years` of simulation,
+    outside the timed region."""
+    import ctypes as C
+    from fastiso_b200 import abi
+
+    if sim.stats()["executor"] != abi.FI_EXEC_PERSIST:
+        return None
+    lib, h = sim.lib, sim._handle
+    if lib.fi_trace_phases(h, 1):
+        return None
+    F.step(integ, years, True)
+    ms = (C.c_double * abi.FI_NUM_PHASES)()
+    cnt = (C.c_int64 * abi.FI_NUM_PHASES)()
+    lib.fi_get_phase_trace(h, ms, cnt)
+    lib.fi_trace_phases(h, 0)
+    out = {}
+    for name, t, c in zip(abi.PHASE_NAMES, ms, cnt):
+        if c:
+            out[name] = {"us": round(1e3 * t / c, 3), "count": int(c)}
+    return out
+
+
 def bytes_per_launch(nx, ny):
     """Algorithmic bytes of each fused kernel (stage-2 variants as timed): every input
     read once, every output written once, halo re-reads and twiddles not counted."""
@@ -247,6 +271,7 @@ def run_gpu(args, rank, world, dev):
         if world > 1:
             torch.distributed.barrier()
     c1 = counters(sim)
+    phases = phase_timeline(sim, integ) if rank == 0 else None
     t_total = float(sum(step_ms))
     if world > 1:
         tt = torch.tensor([t_total], dtype=torch.float64, device=f"cuda:{dev}")
@@ -330,6 +355,7 @@ def run_gpu(args, rank, world, dev):
                 "d2h_bytes_per_step": 8 * N350 * N350,
                 "path": "init_integrator + per step: set H_ice (host) -> step!(1 kyr) -> read u (host)"},
         "gpu_launches": int(launches),
+        "phases": phases,
         "roofline": roof,
         "cpu_baseline": {"value": cpu_v, "unit": "kyr/s", "cores": cores, "kind": "port",
                          "sample": f"FP64 oracle (C, OpenMP), config2 N=350, {yrs:g} yr from t=0"},

@@ -6,7 +6,7 @@ update_diagnostics!) over the C ABI of libfastiso_b200.so (include/fastiso_b200.
 """
 from . import abi  # noqa: F401
 from .model import (  # noqa: F401
-    BoundaryConditions, CompressibleLithosphereColumn, CompressibleMantle, ConstantBSL, CornerBC, DiffEqOptions,
+    BoundaryConditions, CompressibleLithosphereColumn, CompressibleMantle, ConstantBSL, CornerBC, DiffEqOptions, Ensemble,
     ExtendedBCSpace, ExternallyUpdatedIceThickness, FreqDomainViscosityLumping, IncompressibleLithosphereColumn,
     IncompressibleMantle, Integrator, LaterallyConstantSeaSurface, LaterallyVariableLithosphere,
     LaterallyVariableSeaSurface, MaxwellMantle, NativeOutput, NoCalibration, NoSealevelLoad, PhysicalConstants,

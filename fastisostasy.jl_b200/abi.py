@@ -38,6 +38,12 @@ FI_COLUMN_INCOMPRESSIBLE = 0
 FI_COLUMN_COMPRESSIBLE = 1
 FI_ICE_TIME_INTERPOLATED = 0
 FI_ICE_EXTERNAL = 1
+FI_EXEC_PERSIST = 0
+FI_EXEC_GRAPH = 1
+FI_EXEC_LOOP = 2
+FI_NUM_PHASES = 11
+PHASE_NAMES = ("conv_rows", "conv_cols", "conv_rows_inv", "rows_fwd2", "cols2", "rows_fwd3", "cols3", "rows_fwd4",
+               "cols4", "rows_inv4", "controller")
 
 FIELDS = {
     "litho_rigidity": 0,
@@ -123,6 +129,8 @@ class FiStats(C.Structure):
         ("gpu_ms", C.c_double),
         ("last_gpu_ms", C.c_double),
         ("segments", C.c_int64),
+        ("executor", C.c_int32),
+        ("grid", C.c_int32),
     ]
 
 
@@ -203,6 +211,12 @@ _SIGS = {
     "fi_checkpoint": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]),
     "fi_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "fi_time_kernels": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "fi_trace_phases": (C.c_int, [C.c_void_p, C.c_int32]),
+    "fi_get_phase_trace": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "fi_ensemble_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
+    "fi_ensemble_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int32)]),
+    "fi_ensemble_last_gpu_ms": (C.c_double, [C.c_void_p]),
+    "fi_ensemble_destroy": (None, [C.c_void_p]),
     "fi_last_error": (C.c_char_p, [C.c_void_p]),
     "fi_status_string": (C.c_char_p, [C.c_int32]),
     "fi_destroy": (None, [C.c_void_p]),

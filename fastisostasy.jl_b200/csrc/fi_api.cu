@@ -18,6 +18,7 @@
 #include "fi_device.cuh"
 #include "fi_kernels.h"
 #include "fi_noalloc.cuh"
+#include "fi_phases.cuh"
 #include "fi_plain.h"
 
 using namespace fi;
@@ -25,6 +26,7 @@ using namespace fi;
 namespace {
 
 constexpr int NT = 256;
+enum { EXEC_PERSIST = FI_EXEC_PERSIST, EXEC_GRAPH = FI_EXEC_GRAPH, EXEC_LOOP = FI_EXEC_LOOP };
 
 inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
@@ -78,6 +80,7 @@ struct fi_handle {
     Task *t_rows = nullptr, *t_cols = nullptr, *t_crow = nullptr, *t_ccol = nullptr, *t_crowi = nullptr;
     int n_rows, n_cols, n_crow, n_ccol, n_crowi;
     int h_rows = 2, B_cols = 2, h_conv = 2, B_conv = 1;
+    int stage_inputs = 0;  // forward row inputs: 1 = async copies into shared memory, 0 = in place
     double* d_uin = nullptr;
     float* d_vscr = nullptr;
     double* d_cscr = nullptr;
@@ -87,6 +90,14 @@ struct fi_handle {
     cudaGraphExec_t seg_exec = nullptr;
     cudaGraph_t seg_graph = nullptr;
     bool graph_ok = true;
+    // step executor of the fused form: persistent cooperative kernel, CUDA graph, or
+    // host-driven loop of per-phase launches (FI_EXECUTOR=persist|graph|loop)
+    int executor = EXEC_PERSIST;
+    unsigned int* d_bar = nullptr;
+    PersistArgs pargs{};
+    int persist_grid = 0;
+    size_t persist_smem = 0;
+    unsigned long long* d_trace = nullptr;  // phase timeline of the persistent executor
     // plain form
     PlainBufs p{};
     // integrator (host mirror for the plain form; snapshot for the fused form)
@@ -290,8 +301,12 @@ int fi_create(const fi_config* cfg, fi_handle** out) {
         delete h;
         return FI_ERR_CUDA;
     }
+    const char* ex = getenv("FI_EXECUTOR");
+    if (ex && !strcmp(ex, "graph")) h->executor = EXEC_GRAPH;
+    if (ex && !strcmp(ex, "loop")) h->executor = EXEC_LOOP;
     const char* ng = getenv("FI_NO_GRAPH");
-    if (ng && ng[0] == '1') h->graph_ok = false;  // host-driven step loop (profiling / debugging)
+    if (ng && ng[0] == '1') h->executor = EXEC_LOOP;
+    if (h->executor == EXEC_LOOP) h->graph_ok = false;
     int rc = create_buffers(h);
     if (!rc && (cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)) rc = FI_ERR_CUDA;
     if (rc) {
@@ -377,7 +392,8 @@ static int create_buffers(fi_handle* h) {
         RET(dalloc(h, &m.dz, n));
         RET(dalloc(h, &m.sig_load, n));
         RET(dalloc(h, &m.sig_geo, n));
-        RET(dalloc(h, &m.S, (size_t)h->ny * h->sp));
+        RET(dalloc(h, &m.S[0], (size_t)h->ny * h->sp));
+        RET(dalloc(h, &m.S[1], (size_t)h->ny * h->sp));
         RET(dalloc(h, &m.SA, (size_t)h->ny * h->msp));
         RET(dalloc(h, &m.SB, (size_t)h->ny * h->msp));
         RET(dalloc(h, &m.TA, (size_t)(h->ny + 2) * h->msp));
@@ -386,7 +402,10 @@ static int create_buffers(fi_handle* h) {
         RET(dalloc(h, &GA, (size_t)h->MH * h->My)); m.GA = GA;
         RET(dalloc(h, &GB, (size_t)h->MH * h->My)); m.GB = GB;
         RET(dalloc(h, &m.partial, (size_t)h->ny + 16));
+        RET(dalloc(h, &m.cpart, (size_t)4 * (h->NH + 16)));
         RET(dalloc(h, &h->d_ctl, 1));
+        RET(dalloc(h, &h->d_bar, 4));
+        RET(dalloc(h, &h->d_trace, 2 * PH_COUNT));
         m.ctl = h->d_ctl;
         m.tout = h->d_tout;
         RET(dalloc(h, &h->d_uin, n));
@@ -396,6 +415,9 @@ static int create_buffers(fi_handle* h) {
         // tunables
         h->h_rows = 2;
         h->B_cols = h->ny >= 768 ? 1 : 2;
+        if (const char* e = getenv("FI_H_ROWS")) h->h_rows = std::max(1, std::min(8, atoi(e)));
+        if (const char* e = getenv("FI_B_COLS")) h->B_cols = std::max(1, std::min(8, atoi(e)));
+        if (const char* e = getenv("FI_STAGE_INPUTS")) h->stage_inputs = atoi(e) ? 1 : 0;
         h->h_conv = h->Mx >= 1024 ? 1 : 2;
         h->B_conv = 1;
         h->n_rows = cdiv(h->ny, h->h_rows);
@@ -620,6 +642,8 @@ static int build_kernel_spectrum(fi_handle* h, const double* G, float2* half32, 
 }
 
 static int rhs_fused(fi_handle* h, int stage, const double* uin, float* vout, double* cout);
+static int setup_persist(fi_handle* h, int K);
+static int plan_layouts(fi_handle* h, int K);
 static int rhs_plain(fi_handle* h, double t, double* u, double* dudt);
 
 extern "C" int fi_init(fi_handle* h) {
@@ -691,12 +715,6 @@ extern "C" int fi_init(fi_handle* h) {
     ct.t_stop = c.t1;
     if (c.form == FI_FORM_FP32) {
         const int K = (int)h->ice_t.size();
-        const size_t need[] = {rows_fwd_smem(h->nx, h->h_rows, 1, K), cols_smem(h->ny, h->B_cols),
-                               rows_inv_smem(h->nx, h->h_rows), conv_rows_smem(h->Mx, h->h_conv),
-                               conv_cols_smem(h->My, h->B_conv)};
-        for (size_t q : need)
-            if (q + sizeof(fi::Member) + sizeof(fi::Ctl) + 4096 > h->smem_cap)
-                return set_err(h, FI_ERR_ARG, "shared memory need %zu B exceeds the per-block limit", q);
         Member& m = h->mem;
         m.dx = h->dx; m.dy = h->dy; m.A = h->dx * h->dy;
         m.g = c.g; m.rho_ice = c.rho_ice; m.rho_litho = c.rho_litho; m.rho_um = c.rho_uppermantle;
@@ -724,6 +742,8 @@ extern "C" int fi_init(fi_handle* h) {
         m.flags = (any_mask ? FLAG_MASK : 0) | (any_haf ? FLAG_HAFREF : 0) | (any_sig ? FLAG_SIGREF : 0) |
                   (zb_uniform ? 0 : FLAG_ZBSS) | (any_ueref ? FLAG_UEREF : 0);
         m.zbss_scalar = (float)zbss[0];
+        m.ncols = h->n_cols;
+        RET(plan_layouts(h, K));
         RET(upload(h, (float*)m.D, h->D));
         RET(upload(h, (float*)m.visc_fac, vf));
         RET(upload(h, (float*)m.mask, h->mask));
@@ -813,14 +833,14 @@ static int launch_sparse(fi_handle* h) {
 static int launch_rhs_body(fi_handle* h, int stage, const double* uin, float* vout, double* cout,
                            cudaGraphConditionalHandle hg, cudaGraphConditionalHandle hw) {
     const int inv = (stage == 3 || stage == 4) ? 1 : 0;
-    k_rows_fwd<<<h->n_rows, ROW_THREADS, rows_fwd_smem(h->nx, h->h_rows, inv, (int)h->ice_t.size()), h->stream>>>(
+    k_rows_fwd<<<h->n_rows, ROW_THREADS, rows_fwd_smem(h->mem.fl.bytes, h->nx, (int)h->ice_t.size()), h->stream>>>(
         h->d_mem, h->t_rows, stage, h->h_rows, uin, inv);
     CKL();
     const int next = (stage == 2 || stage == 3) ? stage + 1 : 0;
     k_cols<<<h->n_cols, ROW_THREADS, cols_smem(h->ny, h->B_cols), h->stream>>>(h->d_mem, h->t_cols, h->B_cols, next, 0);
     CKL();
     if (stage <= 1 || stage == 4) {
-        k_rows_inv<<<h->n_rows, ROW_THREADS, rows_inv_smem(h->nx, h->h_rows), h->stream>>>(
+        k_rows_inv<<<h->n_rows, ROW_THREADS, rows_inv_smem(h->nx, h->h_rows, h->n_cols), h->stream>>>(
             h->d_mem, h->t_rows, stage, h->h_rows, vout, cout, hg, hw);
         CKL();
     }
@@ -1209,21 +1229,108 @@ static int build_segment_graph(fi_handle* h) {
         double* cout = nullptr;
         cudaGraphConditionalHandle hnext = (s < 4) ? hg[s - 1] : 0;
         void* a1[] = {(void*)&mp, (void*)&tr, (void*)&stage, (void*)&hr, (void*)&uin, (void*)&inv};
-        RET(add_kernel(h, body, &bp, (void*)k_rows_fwd, h->n_rows, rows_fwd_smem(h->nx, hr, inv, (int)h->ice_t.size()), a1));
+        RET(add_kernel(h, body, &bp, (void*)k_rows_fwd, h->n_rows, rows_fwd_smem(h->mem.fl.bytes, h->nx, (int)h->ice_t.size()), a1));
         void* a2[] = {(void*)&mp, (void*)&tc, (void*)&bcol, (void*)&next, (void*)&hnext};
         RET(add_kernel(h, body, &bp, (void*)k_cols, h->n_cols, cols_smem(h->ny, bcol), a2));
         if (s == 4) {
             cudaGraphConditionalHandle hgate = hg[0], hloop = hw;
             void* a3[] = {(void*)&mp, (void*)&tr, (void*)&stage, (void*)&hr,
                           (void*)&vout, (void*)&cout, (void*)&hgate, (void*)&hloop};
-            RET(add_kernel(h, body, &bp, (void*)k_rows_inv, h->n_rows, rows_inv_smem(h->nx, hr), a3));
+            RET(add_kernel(h, body, &bp, (void*)k_rows_inv, h->n_rows, rows_inv_smem(h->nx, hr, h->n_cols), a3));
         }
     }
     CK(cudaGraphInstantiate(&h->seg_exec, g, 0));
     return FI_OK;
 }
 
+// Shared-memory budget of the row phases: the forward row staging layout is sized so
+// that two persistent blocks fit on an SM (one if two cannot), then checked against the
+// per-block limit of the per-phase kernels.
+static int plan_layouts(fi_handle* h, int K) {
+    Member& m = h->mem;
+    int smem_sm = 0;
+    CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->cfg.device));
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, k_persist));
+    const long long extra = (long long)(h->nx + h->ny) * (long long)sizeof(float2) + (K <= TICE_MAX ? 8LL * K : 0);
+    const size_t others[] = {ws_cols(h->ny, h->B_cols), ws_rows_inv(h->nx, h->h_rows, h->n_cols),
+                             ws_conv_rows(h->Mx, h->h_conv), ws_conv_cols(h->My, h->B_conv)};
+    long long other_max = 0;
+    for (size_t q : others) other_max = std::max(other_max, (long long)q);
+    bool fits = false;
+    for (int target = 2; target >= 1 && !fits; target--) {
+        const long long budget = (long long)smem_sm / target - (long long)fa.sharedSizeBytes - 1024 - extra;
+        if (budget <= 0) continue;
+        fwd_layout(h->nx, h->h_rows, m.flags, h->n_cols, (size_t)budget, h->stage_inputs, &m.fl);
+        fits = m.fl.bytes <= budget && other_max <= budget;
+    }
+    if (!fits) {
+        fwd_layout(h->nx, h->h_rows, m.flags, h->n_cols, 0, 0, &m.fl);
+        if (h->executor == EXEC_PERSIST) h->executor = EXEC_GRAPH;
+    }
+    const size_t need[] = {rows_fwd_smem(m.fl.bytes, h->nx, K), cols_smem(h->ny, h->B_cols),
+                           rows_inv_smem(h->nx, h->h_rows, h->n_cols), conv_rows_smem(h->Mx, h->h_conv),
+                           conv_cols_smem(h->My, h->B_conv)};
+    for (size_t q : need)
+        if (q + sizeof(fi::Member) + sizeof(fi::Ctl) + 4096 > h->smem_cap)
+            return set_err(h, FI_ERR_ARG, "shared memory need %zu B exceeds the per-block limit", q);
+    return setup_persist(h, K);
+}
+
+// Persistent executor set-up: shared-memory layout, grid = resident blocks (at most
+// two per SM), cooperative launch support.  Falls back to the graph executor.
+static int setup_persist(fi_handle* h, int K) {
+    if (h->executor != EXEC_PERSIST) return FI_OK;
+    PersistArgs& a = h->pargs;
+    unsigned long long* trace = a.trace;
+    a = PersistArgs{};
+    a.trace = trace;
+    a.mem = h->d_mem;
+    a.bar = h->d_bar;
+    a.h_rows = h->h_rows; a.B_cols = h->B_cols; a.h_conv = h->h_conv; a.B_conv = h->B_conv;
+    a.n_rows = h->n_rows; a.n_cols = h->n_cols; a.n_crow = h->n_crow; a.n_ccol = h->n_ccol; a.n_crowi = h->n_crowi;
+    const size_t smem = persist_layout(h->nx, h->ny, h->Mx, h->My, K, h->mem.fl.bytes, h->h_rows, h->n_cols, h->B_cols,
+                                       h->h_conv, h->B_conv, &a);
+    int coop = 0, nsm = 0, occ = 0;
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->cfg.device));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->cfg.device));
+    if (!coop || smem + 8192 > h->smem_cap) {
+        h->executor = EXEC_GRAPH;
+        return FI_OK;
+    }
+    CK(cudaFuncSetAttribute(k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persist, ROW_THREADS, smem));
+    if (occ < 1) {
+        h->executor = EXEC_GRAPH;
+        return FI_OK;
+    }
+    h->persist_grid = nsm * std::min(occ, 2);
+    h->persist_smem = smem;
+    return FI_OK;
+}
+
+static int run_segment_persist(fi_handle* h) {
+    CK(cudaMemsetAsync(h->d_bar, 0, 4 * sizeof(unsigned int), h->stream));
+    void* args[] = {(void*)&h->pargs};
+    CK(cudaLaunchCooperativeKernel((const void*)k_persist, dim3(h->persist_grid), dim3(ROW_THREADS), args,
+                                   h->persist_smem, h->stream));
+    unsigned int bar[4];
+    CK(cudaMemcpyAsync(bar, h->d_bar, sizeof(bar), cudaMemcpyDeviceToHost, h->stream));
+    RET(read_ctl(h));
+    if (bar[2]) return set_err(h, FI_ERR_TIMEOUT, "persistent step kernel: a grid barrier wait gave up");
+    return FI_OK;
+}
+
+// Launches one segment of the graph executor without waiting (the ensemble driver
+// overlaps the members' segments on their streams).
+static int launch_segment_graph_async(fi_handle* h) {
+    if (!h->seg_exec) RET(build_segment_graph(h));
+    CK(cudaGraphLaunch(h->seg_exec, h->stream));
+    return FI_OK;
+}
+
 static int run_segment_fused(fi_handle* h) {
+    if (h->executor == EXEC_PERSIST) return run_segment_persist(h);
     if (h->graph_ok && !h->seg_exec) {
         if (build_segment_graph(h) != FI_OK) {
             // conditional graph nodes unavailable: use the host loop
@@ -1471,6 +1578,148 @@ extern "C" int fi_step(fi_handle* h, double dt) {
     return rc;
 }
 
+// ---------------------------------------------------------------------------
+// batched ensembles: the members' step loops run concurrently on their own streams
+// ---------------------------------------------------------------------------
+struct fi_ensemble {
+    std::vector<fi_handle*> mem;
+    std::vector<cudaEvent_t> ev_start, ev_end;
+    double last_gpu_ms = 0.0;
+    std::string err;
+};
+
+extern "C" int fi_ensemble_create(fi_handle* const* members, int32_t n, fi_ensemble** out) {
+    if (!members || n < 1 || !out) return FI_ERR_ARG;
+    *out = nullptr;
+    const int dev = members[0]->cfg.device;
+    for (int i = 0; i < n; i++) {
+        fi_handle* h = members[i];
+        if (!h || h->cfg.form != FI_FORM_FP32 || h->cfg.device != dev) return FI_ERR_ARG;
+        if (!h->integ_started) return FI_ERR_STATE;
+        for (int j = 0; j < i; j++)
+            if (members[j] == h) return FI_ERR_ARG;
+    }
+    cudaSetDevice(dev);
+    fi_ensemble* e = new fi_ensemble();
+    e->mem.assign(members, members + n);
+    e->ev_start.resize(n);
+    e->ev_end.resize(n);
+    for (int i = 0; i < n; i++) {
+        // each member's step loop is a CUDA graph (the persistent executor assumes the
+        // whole GPU); the members' graphs overlap on their streams
+        fi_handle* h = e->mem[i];
+        if (h->executor == EXEC_PERSIST) h->executor = EXEC_GRAPH;
+        if (cudaEventCreate(&e->ev_start[i]) != cudaSuccess || cudaEventCreate(&e->ev_end[i]) != cudaSuccess) {
+            fi_ensemble_destroy(e);
+            return FI_ERR_CUDA;
+        }
+    }
+    *out = e;
+    return FI_OK;
+}
+
+void fi_ensemble_destroy(fi_ensemble* e) {
+    if (!e) return;
+    if (!e->mem.empty()) cudaSetDevice(e->mem[0]->cfg.device);
+    for (cudaEvent_t ev : e->ev_start)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : e->ev_end)
+        if (ev) cudaEventDestroy(ev);
+    delete e;
+}
+
+// One member's completion of a launched segment (the tail of solve_until_).
+static int ensemble_finish_segment(fi_handle* h) {
+    RET(read_ctl(h));
+    h->segments += 1;
+    Ctl& ct = h->ctl;
+    if (ct.status != FI_OK)
+        return set_err(h, ct.status, "integration stopped at t=%.6g: %s", ct.t, fi_status_string(ct.status));
+    if (ct.pending_output) {
+        ct.kout += 1;
+        ct.pending_output = 0;
+        RET(write_ctl(h));
+        h->fsal_pending = true;
+    }
+    while (!h->tstops.empty() && h->ctl.t == h->tstops.front()) h->tstops.erase(h->tstops.begin());
+    if (!h->tstops.empty() && h->ctl.t > h->tstops.front())
+        return set_err(h, FI_ERR_STATE, "integrator stepped past a tstop");
+    return FI_OK;
+}
+
+static int ensemble_launch_segment(fi_handle* h) {
+    if (h->fsal_pending) {
+        RET(reeval_fsal(h));
+        h->fsal_pending = false;
+        if (h->ctl.status != FI_OK) return set_err(h, h->ctl.status, "%s", fi_status_string(h->ctl.status));
+    }
+    RET(read_ctl(h));
+    h->ctl.t_stop = h->tstops.front();
+    RET(write_ctl(h));
+    return launch_segment_graph_async(h);
+}
+
+extern "C" int fi_ensemble_step(fi_ensemble* e, double dt, int32_t* status) {
+    if (!e || !(dt > 0)) return FI_ERR_ARG;
+    const int n = (int)e->mem.size();
+    cudaSetDevice(e->mem[0]->cfg.device);
+    std::vector<std::vector<double>> rest(n);
+    std::vector<int> st(n, FI_OK), state(n, 0);  // state: 0 idle, 1 launched, 2 done
+    for (int i = 0; i < n; i++) {
+        fi_handle* h = e->mem[i];
+        int rc = read_ctl(h);
+        const double next_t = h->ctl.t + dt;
+        if (!rc && next_t > h->cfg.t1) rc = set_err(h, FI_ERR_ARG, "step beyond t_span");
+        if (rc) { st[i] = rc; state[i] = 2; continue; }
+        std::vector<double>& v = h->tstops;
+        v.insert(std::lower_bound(v.begin(), v.end(), next_t), next_t);
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        while (!v.empty() && v.back() > next_t) { rest[i].insert(rest[i].begin(), v.back()); v.pop_back(); }
+        if (cudaEventRecord(e->ev_start[i], h->stream) != cudaSuccess) { st[i] = FI_ERR_CUDA; state[i] = 2; }
+    }
+    for (;;) {
+        bool any = false;
+        for (int i = 0; i < n; i++) {
+            if (state[i] != 0) continue;
+            fi_handle* h = e->mem[i];
+            if (h->tstops.empty()) { state[i] = 2; continue; }
+            const int rc = ensemble_launch_segment(h);
+            if (rc) { st[i] = rc; state[i] = 2; continue; }
+            state[i] = 1;
+            any = true;
+        }
+        if (!any) break;
+        for (int i = 0; i < n; i++) {
+            if (state[i] != 1) continue;
+            const int rc = ensemble_finish_segment(e->mem[i]);
+            state[i] = rc ? 2 : 0;
+            if (rc) st[i] = rc;
+        }
+    }
+    float ms = 0.0f, t_first = 0.0f, t_last = 0.0f;
+    bool timed = false;
+    for (int i = 0; i < n; i++) {
+        fi_handle* h = e->mem[i];
+        h->tstops.insert(h->tstops.end(), rest[i].begin(), rest[i].end());
+        h->last_call = 0;
+        if (cudaEventRecord(e->ev_end[i], h->stream) != cudaSuccess) continue;
+        if (cudaEventSynchronize(e->ev_end[i]) != cudaSuccess) continue;
+        float a = 0.0f, b = 0.0f;
+        if (cudaEventElapsedTime(&a, e->ev_start[0], e->ev_start[i]) != cudaSuccess) continue;
+        if (cudaEventElapsedTime(&b, e->ev_start[0], e->ev_end[i]) != cudaSuccess) continue;
+        if (!timed) { t_first = a; t_last = b; timed = true; }
+        t_first = std::min(t_first, a);
+        t_last = std::max(t_last, b);
+    }
+    if (timed) ms = t_last - t_first;
+    e->last_gpu_ms = ms;
+    if (status)
+        for (int i = 0; i < n; i++) status[i] = st[i];
+    return FI_OK;
+}
+
+extern "C" double fi_ensemble_last_gpu_ms(const fi_ensemble* e) { return e ? e->last_gpu_ms : 0.0; }
+
 extern "C" int fi_get_stats(fi_handle* h, fi_stats* st) {
     if (h) cudaSetDevice(h->cfg.device);
     if (!h || !st) return FI_ERR_ARG;
@@ -1488,6 +1737,8 @@ extern "C" int fi_get_stats(fi_handle* h, fi_stats* st) {
     st->gpu_ms = h->gpu_ms;
     st->last_gpu_ms = h->last_gpu_ms;
     st->segments = h->segments;
+    st->executor = h->cfg.form == FI_FORM_FP32 ? h->executor : -1;
+    st->grid = h->executor == EXEC_PERSIST ? h->persist_grid : 0;
     return FI_OK;
 }
 
@@ -1506,7 +1757,7 @@ extern "C" int fi_time_kernels(fi_handle* h, int32_t reps, double* ms) {
             if (r == 0) CK(cudaEventRecord(h->ev0, h->stream));
             switch (k) {
                 case 0:
-                    k_rows_fwd<<<h->n_rows, ROW_THREADS, rows_fwd_smem(h->nx, h->h_rows, 1, (int)h->ice_t.size()), h->stream>>>(
+                    k_rows_fwd<<<h->n_rows, ROW_THREADS, rows_fwd_smem(h->mem.fl.bytes, h->nx, (int)h->ice_t.size()), h->stream>>>(
                         h->d_mem, h->t_rows, 3, h->h_rows, nullptr, 1);
                     break;
                 case 1:
@@ -1514,7 +1765,7 @@ extern "C" int fi_time_kernels(fi_handle* h, int32_t reps, double* ms) {
                         h->d_mem, h->t_cols, h->B_cols, 0, 0);
                     break;
                 case 2:
-                    k_rows_inv<<<h->n_rows, ROW_THREADS, rows_inv_smem(h->nx, h->h_rows), h->stream>>>(
+                    k_rows_inv<<<h->n_rows, ROW_THREADS, rows_inv_smem(h->nx, h->h_rows, h->n_cols), h->stream>>>(
                         h->d_mem, h->t_rows, 1, h->h_rows, nullptr, nullptr, 0, 0);
                     break;
                 case 3:
@@ -1537,6 +1788,32 @@ extern "C" int fi_time_kernels(fi_handle* h, int32_t reps, double* ms) {
         float t = 0.0f;
         CK(cudaEventElapsedTime(&t, h->ev0, h->ev1));
         ms[k] = (double)t / reps;
+    }
+    return FI_OK;
+}
+
+static_assert(FI_NUM_PHASES == PH_COUNT, "phase count mismatch");
+
+extern "C" int fi_trace_phases(fi_handle* h, int32_t on) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h) return FI_ERR_ARG;
+    if (h->cfg.form != FI_FORM_FP32) return set_err(h, FI_ERR_UNSUPPORTED, "phase trace is for the FP32 form");
+    if (on) CK(cudaMemsetAsync(h->d_trace, 0, 2 * PH_COUNT * sizeof(unsigned long long), h->stream));
+    h->pargs.trace = on ? h->d_trace : nullptr;
+    CK(cudaStreamSynchronize(h->stream));
+    return FI_OK;
+}
+
+extern "C" int fi_get_phase_trace(fi_handle* h, double* ms, int64_t* counts) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h || !ms || !counts) return FI_ERR_ARG;
+    if (h->cfg.form != FI_FORM_FP32) return set_err(h, FI_ERR_UNSUPPORTED, "phase trace is for the FP32 form");
+    unsigned long long v[2 * PH_COUNT];
+    CK(cudaMemcpyAsync(v, h->d_trace, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int p = 0; p < PH_COUNT; p++) {
+        ms[p] = (double)v[2 * p] * 1e-6;
+        counts[p] = (int64_t)v[2 * p + 1];
     }
     return FI_OK;
 }

@@ -49,9 +49,11 @@ __host__ __device__ inline void loopheader_prep(Ctl* c) {
 }
 
 // PI step-size controller + accept/reject (stepsize_controller!,
-// step_accept_controller!, step_reject_controller!, _loopfooter!).
-// Returns 1 if the step was accepted.  tout: output times (nout_condition).
-__host__ __device__ inline int controller_update(Ctl* c, double EEst, const double* tout) {
+// step_accept_controller!, step_reject_controller!, _loopfooter!), given the two
+// powers EEst^beta1 and qold^beta2.  Returns 1 if the step was accepted.  tout:
+// output times (nout_condition).
+__host__ __device__ inline int controller_update_pw(Ctl* c, double EEst, double q11, double qold_b2,
+                                                    const double* tout) {
     c->EEst = EEst;
     if (!(EEst == EEst)) {
         c->status = FI_ERR_NONFINITE;
@@ -62,8 +64,7 @@ __host__ __device__ inline int controller_update(Ctl* c, double EEst, const doub
     if (EEst == 0.0) {
         q = 1.0 / QMAX;
     } else {
-        const double q11 = pow(EEst, PI_BETA1);
-        q = q11 / pow(c->qold, PI_BETA2);
+        q = q11 / qold_b2;
         c->q11 = q11;
         q = q / GAMMA;
         if (q > 1.0 / QMIN) q = 1.0 / QMIN;
@@ -91,6 +92,11 @@ __host__ __device__ inline int controller_update(Ctl* c, double EEst, const doub
         c->dt /= (1.0 / QMIN < qq ? 1.0 / QMIN : qq);
     }
     return c->accept_step;
+}
+
+__host__ __device__ inline int controller_update(Ctl* c, double EEst, const double* tout) {
+    const bool pw = (EEst == EEst) && EEst != 0.0;
+    return controller_update_pw(c, EEst, pw ? pow(EEst, PI_BETA1) : 0.0, pw ? pow(c->qold, PI_BETA2) : 1.0, tout);
 }
 
 // TimeInterpolation2D lookup (src/interpolations.jl:51-74): snapshot index i and
@@ -149,7 +155,7 @@ __device__ __forceinline__ void block_sum(double* v, double* scratch /* >= 32*NV
 // (normalisation already folded in): the inverse real DFT evaluated directly.
 // Partial sums of this thread over k = tid, tid+nth, ...
 template <typename C, typename T>
-__device__ __forceinline__ void row_corner_partial(const C* __restrict__ A, int nx, const T* __restrict__ twr,
+__device__ __forceinline__ void row_corner_partial(const C* A, int nx, const T* __restrict__ twr,
                                                    double* v0, double* v1) {
     // twr: forward twiddles exp(-2 pi i k / nx) as (re, im) pairs
     const int kmax = (nx - 1) / 2;

@@ -58,6 +58,22 @@ struct Ctl {
     unsigned int arrive_pad;
 };
 
+// Shared-memory layout of the forward row phase: byte offsets (16-byte aligned) of the
+// staging buffers of one row tile.  An input whose offset is -1 is read in place from
+// global memory (the layout is budgeted per member; results do not depend on it).
+struct FwdLayout {
+    int U;        // stage vector rows [loU, hiU), FP64 (prefetched uprev, updated in place)
+    int MS;       // moments (3 x capM rows, FP32), aliased by the inverse-prologue FFT
+    int KA, KB, KC;  // k1, k2, k3 rows [loU, hiU) (FP32)
+    int S_in;     // previous stage's spectrum rows [loU, hiU) (complex)
+    int D;        // rigidity rows [loM, hiM)
+    int Ha, Hb, ue, uz, dz, visc, zbss, mask, hafref, sigref, ueref;  // own rows
+    int R;        // -g sigma_full of the own rows
+    int cpart;    // corner partials of the column tasks (4 doubles each)
+    int stage_u;  // 1: uprev rows are copied into U asynchronously; 0: read in place
+    int bytes;
+};
+
 // Per-member static description + device pointers.
 struct Member {
     int nx, ny, NH, sp;         // grid, half-spectrum width nx/2+1, spectrum row pitch
@@ -74,7 +90,8 @@ struct Member {
     double border_v, border_e, border_g;
     double dt_sparse;
     float zbss_scalar;
-    float pad1;
+    int ncols;                  // column tasks (corner partials per right-hand side)
+    FwdLayout fl;               // forward row phase staging layout
     // state
     double* u[2];               // FP64 state double buffer
     float* k14[2];              // k1 / k4 physical (raw, before the corner offset)
@@ -96,7 +113,7 @@ struct Member {
     float* dz;                  // raw sea-surface perturbation
     float* sig_load;            // columnanoms.load of the last RHS call
     float* sig_geo;             // sea-surface convolution input of the last RHS call
-    float2* S;                  // viscous half spectrum [ny][sp]
+    float2* S[2];               // viscous half spectrum [ny][sp], double-buffered (stage 3 uses S[1])
     float2* SA;                 // convolution spectrum, channel A [ny][msp]
     float2* SB;                 // convolution spectrum, channel B [ny][msp]
     float2* TA;                 // cropped column output, channel A [ny+2][msp]
@@ -104,6 +121,7 @@ struct Member {
     const float2* GA;           // kernel spectrum channel A [MH][My] (kx-major)
     const float2* GB;
     double* partial;            // error-norm partial sums per row tile
+    double* cpart;              // corner partials [ncols][4] of the last column pass
     const double* tout;         // output times (nout_condition), ctl->nout entries
     Ctl* ctl;
 };

@@ -24,12 +24,34 @@ __global__ void kf_initdt_u1(double* u1, const double* u, const float* v, const 
 __global__ void kf_initdt_d2(const double* u, const float* v0, const double* c0p, const float* v1,
                              const double* c1p, double border, double abstol, double reltol, double* partial,
                              size_t n);
-size_t rows_fwd_smem(int nx, int h, int inv, int K);
+size_t rows_fwd_smem(int ws_bytes, int nx, int K);
 constexpr int ROW_THREADS = 512;
 size_t cols_smem(int ny, int B);
-size_t rows_inv_smem(int nx, int h);
+size_t rows_inv_smem(int nx, int h, int ncols);
 size_t conv_rows_smem(int Mx, int h);
 size_t conv_cols_smem(int My, int B);
+
+// ---- persistent step executor (fi_persist.cu) ----
+struct PersistArgs {
+    const Member* mem;
+    unsigned int* bar;  // grid barrier: [0] arrivals, [1] generation, [2] abort
+    int h_rows, B_cols, h_conv, B_conv;
+    int n_rows, n_cols, n_crow, n_ccol, n_crowi;
+    int ws_bytes;       // phase workspace at the front of dynamic shared memory
+    int tw_off[4];      // float2 offsets (after the workspace) of the x, y, Mx, My twiddles; -1: global
+    int tice_off;       // float2 offset of the ice-time table, -1: read from global memory
+    unsigned long long* trace;  // optional phase timeline: [2 * PH_COUNT] sums of ns and counts
+};
+// phases of the persistent executor, as accumulated in PersistArgs::trace
+enum {
+    PH_CONV_ROWS = 0, PH_CONV_COLS, PH_CONV_ROWS_INV,
+    PH_ROWS_FWD2, PH_COLS2, PH_ROWS_FWD3, PH_COLS3, PH_ROWS_FWD4, PH_COLS4, PH_ROWS_INV4, PH_CONTROLLER,
+    PH_COUNT
+};
+__global__ void k_persist(PersistArgs a);
+// fills the shared-memory layout fields of a and returns the dynamic shared memory bytes
+size_t persist_layout(int nx, int ny, int Mx, int My, int K, int fwd_bytes, int h_rows, int ncols, int B_cols,
+                      int h_conv, int B_conv, PersistArgs* a);
 
 // ---- FP64 transforms and set-up (fi_setup.cu) ----
 __global__ void k_fft64_rows(double2* a, int nx, int ny, int pitch, const FftPlan* plans, int plan, int inverse,

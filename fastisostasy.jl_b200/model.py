@@ -595,3 +595,51 @@ def step(integrator: Integrator, dt, force_dt=True):
         raise UnsupportedError("step! is always used with force_dt = true")
     sim = integrator.sim
     sim._check(sim.lib.fi_step(sim._handle, float(dt)), "fi_step")
+
+
+class Ensemble:
+    """Batched ensemble of FP32 simulations stepped together (no counterpart in the
+    reference; its only batching is the host-threaded ensemble of
+    ext/FastIsostasyEnsembleKalmanProcessesExt.jl:107-122).  Each member keeps its own
+    grid, fields and integrator; ``step(dt)`` is ``step!(integrator_m, dt, true)`` for
+    every member, the members' step loops running concurrently on the GPU.  A member
+    that fails is reported in the returned status list and does not stop the others."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        if not self.sims:
+            raise ValueError("an ensemble needs at least one member")
+        self.integrators = []
+        for s in self.sims:
+            if s.cfg.form != abi.FI_FORM_FP32:
+                raise UnsupportedError("ensemble members use the FP32 form")
+            self.integrators.append(init_integrator(s))
+        self.lib = self.sims[0].lib
+        arr = (C.c_void_p * len(self.sims))(*[s._handle.value for s in self.sims])
+        h = C.c_void_p()
+        rc = self.lib.fi_ensemble_create(arr, len(self.sims), C.byref(h))
+        if rc != abi.FI_OK:
+            raise abi.FiError(rc, "fi_ensemble_create failed")
+        self._h = h
+
+    def step(self, dt):
+        st = (C.c_int32 * len(self.sims))()
+        rc = self.lib.fi_ensemble_step(self._h, float(dt), st)
+        if rc != abi.FI_OK:
+            raise abi.FiError(rc, "fi_ensemble_step failed")
+        return list(st)
+
+    @property
+    def last_gpu_ms(self):
+        return float(self.lib.fi_ensemble_last_gpu_ms(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.fi_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

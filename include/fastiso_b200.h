@@ -131,8 +131,17 @@ typedef struct fi_stats {
     double gpu_ms;            /* device time of integration calls so far (CUDA events on
                                  the handle's stream), ms */
     double last_gpu_ms;       /* device time of the last fi_run / fi_step call, ms */
-    int64_t segments;         /* step-loop launches (one CUDA graph launch each) */
+    int64_t segments;         /* step-loop launches (one per output segment) */
+    int32_t executor;         /* FP32 step executor: FI_EXEC_* */
+    int32_t grid;             /* blocks of the persistent executor (0 otherwise) */
 } fi_stats;
+
+/* Step executors of the FP32 form; the environment variable FI_EXECUTOR
+ * (persist | graph | loop) read by fi_create selects one, default persist.
+ * persist: one cooperative persistent kernel per output segment; graph: a CUDA
+ * graph with conditional nodes, one kernel per phase; loop: the same kernels
+ * launched from a host loop.  All three compute bitwise identical results. */
+enum { FI_EXEC_PERSIST = 0, FI_EXEC_GRAPH = 1, FI_EXEC_LOOP = 2 };
 
 typedef struct fi_handle fi_handle;
 
@@ -218,6 +227,32 @@ int fi_restore(fi_handle* h, const void* buf, size_t size);
  * k_conv_rows, k_conv_cols and k_conv_rows_inv into ms[0..5].  It overwrites the
  * handle's state; use a separate handle. */
 int fi_time_kernels(fi_handle* h, int32_t reps, double* ms);
+
+/* Diagnostics (no counterpart in the reference): phase timeline of the persistent
+ * FP32 executor.  fi_trace_phases(h, 1) clears the sums and starts recording,
+ * fi_trace_phases(h, 0) stops.  fi_get_phase_trace writes FI_NUM_PHASES sums of
+ * time (ms, as seen by block 0: the phase's slowest block plus the grid barrier)
+ * and counts, in the order conv rows, conv columns, conv rows-inverse, rows(2),
+ * columns(2), rows(3), columns(3), rows(4), columns(4), rows-inverse(4) + error
+ * norm, controller. */
+#define FI_NUM_PHASES 11
+int fi_trace_phases(fi_handle* h, int32_t on);
+int fi_get_phase_trace(fi_handle* h, double* ms, int64_t* counts);
+
+/* ---- batched ensembles: no counterpart in the reference (its only batching is the
+ * host-threaded ensemble of ext/FastIsostasyEnsembleKalmanProcessesExt.jl:107-122).
+ * An ensemble groups initialised FP32 handles on one device, each with its own grid,
+ * fields, tolerances and integrator (fi_init_integrator called).  fi_ensemble_step(e,
+ * dt, status) is step!(integrator_m, dt, true) for every member m, with the members'
+ * step loops running concurrently on their streams; status[m] (n entries, may be NULL)
+ * receives each member's FI_* code, and a failing member does not stop the others.
+ * fi_ensemble_last_gpu_ms: device time of the last fi_ensemble_step (first start to
+ * last end over the members' streams).  The ensemble does not own its members. */
+typedef struct fi_ensemble fi_ensemble;
+int fi_ensemble_create(fi_handle* const* members, int32_t n, fi_ensemble** out);
+int fi_ensemble_step(fi_ensemble* e, double dt, int32_t* status);
+double fi_ensemble_last_gpu_ms(const fi_ensemble* e);
+void fi_ensemble_destroy(fi_ensemble* e);
 
 const char* fi_last_error(const fi_handle* h);
 const char* fi_status_string(int32_t status);

@@ -114,13 +114,19 @@ def l2_flush(dev):
 
 def counters(sim):
     st = sim.stats()
-    return {k: st[k] for k in ("nf", "naccept", "nreject", "nsparse", "segments", "gpu_ms")}
+    return {k: st[k] for k in ("nf", "naccept", "nreject", "nsparse", "segments", "gpu_ms", "executor", "grid")}
 
 
-def launches_between(a, b):
-    """Kernels launched by the step loop: 3 per right-hand side (rows_fwd, cols,
-    rows_inv), 3 per sparse update, 1 segment-start per graph launch."""
-    return 3 * (b["nf"] - a["nf"]) + 3 * (b["nsparse"] - a["nsparse"]) + (b["segments"] - a["segments"])
+def launches_between(a, b, executor):
+    """Kernels of this library launched between two counter snapshots.  Persistent
+    executor: one k_persist per segment, plus 7 per host-driven right-hand side (the
+    FSAL re-evaluation after an output: gate, 3 convolution, 3 RHS kernels).  Graph and
+    loop executors: 3 per right-hand side, 3 per sparse update, 1 per segment start."""
+    attempts = (b["naccept"] + b["nreject"]) - (a["naccept"] + a["nreject"])
+    nf = b["nf"] - a["nf"]
+    if executor == 0:
+        return (b["segments"] - a["segments"]) + 7 * max(0, nf - 3 * attempts)
+    return 3 * nf + 3 * (b["nsparse"] - a["nsparse"]) + (b["segments"] - a["segments"])
 
 
 def phase_timeline(sim, integ, years=50.0):
@@ -166,32 +172,90 @@ def bytes_per_launch(nx, ny):
     }
 
 
-def roofline(dev, ms_step, per_step_launch):
+def roofline(dev, us_per_bs3, steps_per_launch, executor, grid):
+    """The persistent step kernel against the HBM roofline: algorithmic bytes of one BS3
+    step (three right-hand sides, each reading its inputs once and writing its outputs
+    once: rows_fwd + cols + rows_inv of bytes_per_launch) times the steps of a launch,
+    over the launch's CUDA-event duration.  The per-phase kernels are timed alone with
+    fi_time_kernels for reference."""
+    import ctypes as C
+
     sim = W.config2(form="fp32", N=N350)
     sim.cfg.device = dev
     F.init_integrator(sim)
-    import ctypes as C
-
     ms = (C.c_double * 6)()
     rc = sim.lib.fi_time_kernels(sim._handle, 200, ms)
+    sim.close()
     if rc:
         raise RuntimeError(f"fi_time_kernels failed ({rc})")
     names = ["k_rows_fwd", "k_cols", "k_rows_inv", "k_conv_rows", "k_conv_cols", "k_conv_rows_inv"]
-    t = dict(zip(names, list(ms)))
-    share = {k: t[k] * per_step_launch[k] for k in names}
-    top = max(share, key=share.get)
     bpl = bytes_per_launch(N350, N350)
+    per_step = 3 * (bpl["k_rows_fwd"] + bpl["k_cols"] + bpl["k_rows_inv"])
     peak, kind = hbm_peak()
-    achieved = bpl[top] / (t[top] * 1e-3) / 1e9
+    achieved = per_step / (us_per_bs3 * 1e-6) / 1e9
     traffic = None
     tpath = ROOT / "profiles" / "roofline_traffic.json"
     if tpath.exists():
-        traffic = json.loads(tpath.read_text()).get(top)
-    sim.close()
-    return {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak, "peak_kind": kind,
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-            "bytes_per_launch": bpl[top], "ms_per_launch": round(t[top], 5),
-            "kernel_ms": {k: round(v, 5) for k, v in t.items()}}
+        per = json.loads(tpath.read_text()).get("k_persist_bytes_per_bs3_step")
+        if per:
+            traffic = round(per * steps_per_launch)
+    return {"bound": "hbm", "kernel": "k_persist" if executor == 0 else "k_rows_fwd/k_cols/k_rows_inv",
+            "achieved": round(achieved, 1), "peak": peak, "peak_kind": kind, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": traffic,
+            "bytes_per_launch": round(per_step * steps_per_launch), "bytes_per_bs3_step": per_step,
+            "bs3_steps_per_launch": steps_per_launch, "grid": grid,
+            "note": "one member's working set is L2-resident within a launch: DRAM traffic is far below the "
+                    "algorithmic bytes and the kernel is latency-bound, not HBM-bound",
+            "phase_kernels_alone_ms": {k: round(v, 5) for k, v in zip(names, list(ms))}}
+
+
+ENS_MEMBERS = 128
+ENS_WINDOW_YR = 1000.0
+
+
+def ensemble_bench(dev):
+    """Config 3: 128 members, N drawn from {64, 96, 128, 192, 256} over N x 30 km, own
+    seeded viscosity fields, shared disc + random-field ice history; the persistent
+    ensemble executor advances all members one window; against looping the plain FP64
+    form member by member (sampled on 4 members)."""
+    members, t_ice, mod = W.config3_members(n_members=ENS_MEMBERS)
+    sims = [W.config3_simulation(m, t_ice, mod, form="fp32") for m in members]
+    for sm in sims:
+        sm.cfg.device = dev
+        sm.cfg.max_steps = 50_000_000
+    ens = F.Ensemble(sims)
+    ens.step(50.0)
+    c0 = [sm.stats() for sm in sims]
+    st = ens.step(ENS_WINDOW_YR)
+    ms = ens.last_gpu_ms
+    c1 = [sm.stats() for sm in sims]
+    steps = [(b["naccept"] + b["nreject"]) - (a["naccept"] + a["nreject"]) for a, b in zip(c0, c1)]
+    rhs = sum(b["nf"] - a["nf"] for a, b in zip(c0, c1))
+    tiles = list(sims[0].tiles) if sims[0].tiles else None
+    ens.close()
+    for sm in sims:
+        sm.close()
+    tot_kyr, tot_ms = 0.0, 0.0
+    for m in members[:4]:
+        ps = W.config3_simulation(m, t_ice, mod, form="fp64")
+        ps.cfg.device = dev
+        ps.cfg.max_steps = 50_000_000
+        pit = F.init_integrator(ps)
+        F.step(pit, 50.0, True)
+        F.step(pit, 200.0, True)
+        tot_kyr += 0.2
+        tot_ms += ps.stats()["last_gpu_ms"]
+        ps.close()
+    v = ENS_MEMBERS * ENS_WINDOW_YR / 1e3 / (ms / 1e3)
+    plain = tot_kyr / (tot_ms / 1e3)
+    return {"value": v, "unit": "member-kyr/s", "members": ENS_MEMBERS,
+            "window": f"{ENS_WINDOW_YR:g} yr after 50 yr (of config 3's 20 kyr)",
+            "tiles": tiles, "status_ok": all(x == 0 for x in st),
+            "steps_per_member": {"min": min(steps), "mean": sum(steps) / len(steps), "max": max(steps)},
+            "rhs_evals_per_s": rhs / (ms / 1e3),
+            "plain_fp64_loop": {"value": plain, "unit": "member-kyr/s",
+                                "sample": "4 members x 200 yr after 50 yr, one after another"},
+            "speedup_vs_plain_loop": v / plain}
 
 
 def cpu_oracle_sample(seconds_target=12.0, seg=5.0):
@@ -280,7 +344,7 @@ def run_gpu(args, rank, world, dev):
     kyr = args.steps * SEG_YR / 1e3
     value = world * kyr / (t_total / 1e3)
     attempts = (c1["naccept"] + c1["nreject"]) - (c0["naccept"] + c0["nreject"])
-    launches = launches_between(c0, c1)
+    launches = launches_between(c0, c1, c1["executor"])
     sim.close()
     if rank != 0:
         return
@@ -322,15 +386,10 @@ def run_gpu(args, rank, world, dev):
     plain_ms_per_bs3 = p1["last_gpu_ms"] / max(1, (p1["naccept"] + p1["nreject"]) - (p0["naccept"] + p0["nreject"]))
     psim.close()
     # ---- roofline of the dominant kernel ----------------------------------------
-    per_step = {"k_rows_fwd": 3, "k_cols": 3, "k_rows_inv": 3, "k_conv_rows": 0, "k_conv_cols": 0,
-                "k_conv_rows_inv": 0}
-    rhs_per_attempt = (c1["nf"] - c0["nf"]) / max(1, attempts)
-    sparse_per_attempt = (c1["nsparse"] - c0["nsparse"]) / max(1, attempts)
-    for k in ("k_rows_fwd", "k_cols", "k_rows_inv"):
-        per_step[k] = rhs_per_attempt
-    for k in ("k_conv_rows", "k_conv_cols", "k_conv_rows_inv"):
-        per_step[k] = sparse_per_attempt
-    roof = roofline(dev, t_total / args.steps, per_step)
+    seg = max(1, c1["segments"] - c0["segments"])
+    roof = roofline(dev, 1e3 * t_total / max(1, attempts), attempts / seg, c1["executor"], c1["grid"])
+    # ---- batched ensemble (config 3) ----------------------------------------------
+    ens = ensemble_bench(dev)
     # ---- CPU baseline (oracle) ---------------------------------------------------
     cpu_v, cores, yrs = cpu_oracle_sample()
     line = {
@@ -350,7 +409,7 @@ def run_gpu(args, rank, world, dev):
         "plain_fp64": {"value": plain_kyr_s, "unit": "kyr/s", "ms_per_bs3_step": plain_ms_per_bs3,
                        "sample": "20 yr after 20 yr warm-up"},
         "speedup_vs_plain_fp64": value / world / plain_kyr_s,
-        "ensemble": None,
+        "ensemble": ens,
         "e2e": {"value": e2e_val, "unit": "kyr/s", "h2d_bytes_per_step": 8 * N350 * N350,
                 "d2h_bytes_per_step": 8 * N350 * N350,
                 "path": "init_integrator + per step: set H_ice (host) -> step!(1 kyr) -> read u (host)"},

@@ -199,6 +199,7 @@ _SIGS = {
     "fi_set_ice_history": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fi_set_elastic_table": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fi_set_channel_scaling": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "fi_set_tiles": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "fi_init": (C.c_int, [C.c_void_p]),
     "fi_rhs": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fi_rhs_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
@@ -216,6 +217,7 @@ _SIGS = {
     "fi_ensemble_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
     "fi_ensemble_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int32)]),
     "fi_ensemble_last_gpu_ms": (C.c_double, [C.c_void_p]),
+    "fi_ensemble_trace": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "fi_ensemble_destroy": (None, [C.c_void_p]),
     "fi_last_error": (C.c_char_p, [C.c_void_p]),
     "fi_status_string": (C.c_char_p, [C.c_int32]),

@@ -336,6 +336,14 @@ void fi_destroy(fi_handle* h) {
 // ---------------------------------------------------------------------------
 // buffers
 // ---------------------------------------------------------------------------
+static void set_task_counts(fi_handle* h) {
+    h->n_rows = cdiv(h->ny, h->h_rows);
+    h->n_cols = cdiv(h->NH, h->B_cols);
+    h->n_crow = cdiv(h->ny, h->h_conv);
+    h->n_ccol = cdiv(h->MH, h->B_conv);
+    h->n_crowi = cdiv(h->ny + 2, h->h_conv);
+}
+
 static int create_buffers(fi_handle* h) {
     const size_t n = N2(h);
     RET(get_plan(h, h->nx, &h->plan_x));
@@ -420,11 +428,8 @@ static int create_buffers(fi_handle* h) {
         if (const char* e = getenv("FI_STAGE_INPUTS")) h->stage_inputs = atoi(e) ? 1 : 0;
         h->h_conv = h->Mx >= 1024 ? 1 : 2;
         h->B_conv = 1;
-        h->n_rows = cdiv(h->ny, h->h_rows);
-        h->n_cols = cdiv(h->NH, h->B_cols);
-        h->n_crow = cdiv(h->ny, h->h_conv);
-        h->n_ccol = cdiv(h->MH, h->B_conv);
-        h->n_crowi = cdiv(h->ny + 2, h->h_conv);
+        set_task_counts(h);
+        // task lists (0, i) sized for the smallest tiles, so fi_set_tiles only changes counts
         auto mk = [&](Task** dst, int count) -> int {
             std::vector<Task> t(count);
             for (int i = 0; i < count; i++) t[i] = Task{0, i};
@@ -433,11 +438,11 @@ static int create_buffers(fi_handle* h) {
             CK(cudaStreamSynchronize(h->stream));
             return FI_OK;
         };
-        RET(mk(&h->t_rows, h->n_rows));
-        RET(mk(&h->t_cols, h->n_cols));
-        RET(mk(&h->t_crow, h->n_crow));
-        RET(mk(&h->t_ccol, h->n_ccol));
-        RET(mk(&h->t_crowi, h->n_crowi));
+        RET(mk(&h->t_rows, h->ny));
+        RET(mk(&h->t_cols, h->NH));
+        RET(mk(&h->t_crow, h->ny));
+        RET(mk(&h->t_ccol, h->MH));
+        RET(mk(&h->t_crowi, h->ny + 2));
         // opt in to the full shared memory per block; the actual need (which depends on the
         // ice-table length) is checked in fi_init
         int smax = 0;
@@ -624,6 +629,19 @@ extern "C" int fi_set_channel_scaling(fi_handle* h, int32_t n, const double* rat
     return FI_OK;
 }
 
+extern "C" int fi_set_tiles(fi_handle* h, int32_t h_rows, int32_t B_cols) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h) return FI_ERR_ARG;
+    if (h->initialized) return set_err(h, FI_ERR_STATE, "fi_set_tiles must precede fi_init");
+    if (h->cfg.form != FI_FORM_FP32) return set_err(h, FI_ERR_UNSUPPORTED, "tiles apply to the FP32 form");
+    if (h_rows < 1 || h_rows > 16 || B_cols < 1 || B_cols > 16)
+        return set_err(h, FI_ERR_ARG, "tile height %d / column block %d outside [1, 16]", h_rows, B_cols);
+    h->h_rows = h_rows;
+    h->B_cols = B_cols;
+    set_task_counts(h);
+    return FI_OK;
+}
+
 // ---------------------------------------------------------------------------
 // set-up (Simulation constructor tail)
 // ---------------------------------------------------------------------------
@@ -743,6 +761,8 @@ extern "C" int fi_init(fi_handle* h) {
                   (zb_uniform ? 0 : FLAG_ZBSS) | (any_ueref ? FLAG_UEREF : 0);
         m.zbss_scalar = (float)zbss[0];
         m.ncols = h->n_cols;
+        m.h_rows = h->h_rows; m.B_cols = h->B_cols; m.h_conv = h->h_conv; m.B_conv = h->B_conv;
+        m.n_rows = h->n_rows; m.n_crow = h->n_crow; m.n_ccol = h->n_ccol; m.n_crowi = h->n_crowi;
         RET(plan_layouts(h, K));
         RET(upload(h, (float*)m.D, h->D));
         RET(upload(h, (float*)m.visc_fac, vf));
@@ -1586,7 +1606,82 @@ struct fi_ensemble {
     std::vector<cudaEvent_t> ev_start, ev_end;
     double last_gpu_ms = 0.0;
     std::string err;
+    // persistent executor (one cooperative launch per segment for all members)
+    bool persist = false;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Member* d_mems = nullptr;
+    Ctl** d_ctls = nullptr;
+    unsigned int* d_bar = nullptr;
+    unsigned long long* d_counter = nullptr;
+    unsigned long long* d_trace = nullptr;
+    EnsArgs args{};
+    int grid = 0;
+    size_t smem = 0;
+    long long launches = 0;
 };
+
+static void ensemble_free(fi_ensemble* e) {
+    if (e->d_mems) cudaFree(e->d_mems);
+    if (e->d_ctls) cudaFree(e->d_ctls);
+    if (e->d_bar) cudaFree(e->d_bar);
+    if (e->d_counter) cudaFree(e->d_counter);
+    if (e->d_trace) cudaFree(e->d_trace);
+    if (e->e0) cudaEventDestroy(e->e0);
+    if (e->e1) cudaEventDestroy(e->e1);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    e->d_mems = nullptr; e->d_ctls = nullptr; e->d_bar = nullptr; e->d_counter = nullptr; e->d_trace = nullptr;
+    e->e0 = e->e1 = nullptr;
+    e->stream = nullptr;
+}
+
+// Persistent ensemble executor set-up; false leaves the stream executor in charge.
+static bool ensemble_setup_persist(fi_ensemble* e) {
+    const char* ex = getenv("FI_ENS_EXECUTOR");
+    if (ex && !strcmp(ex, "streams")) return false;
+    const int n = (int)e->mem.size();
+    if (n > ENS_MAX_MEMBERS) return false;
+    const int dev = e->mem[0]->cfg.device;
+    int coop = 0, nsm = 0, occ = 0, smax = 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return false;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    std::vector<Member> hm(n);
+    std::vector<Ctl*> hc(n);
+    for (int i = 0; i < n; i++) {
+        hm[i] = e->mem[i]->mem;
+        hc[i] = e->mem[i]->d_ctl;
+    }
+    EnsArgs& a = e->args;
+    a = EnsArgs{};
+    const size_t smem = ens_layout(hm.data(), n, &a);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, k_ens) != cudaSuccess) return false;
+    if (smem + fa.sharedSizeBytes + 1024 > (size_t)smax) return false;
+    if (cudaFuncSetAttribute(k_ens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens, ROW_THREADS, smem) != cudaSuccess || occ < 1)
+        return false;
+    const bool okk = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
+                     cudaEventCreate(&e->e0) == cudaSuccess && cudaEventCreate(&e->e1) == cudaSuccess &&
+                     cudaMalloc(&e->d_mems, n * sizeof(Member)) == cudaSuccess &&
+                     cudaMalloc(&e->d_ctls, n * sizeof(Ctl*)) == cudaSuccess &&
+                     cudaMalloc(&e->d_bar, 4 * sizeof(unsigned int)) == cudaSuccess &&
+                     cudaMalloc(&e->d_counter, sizeof(unsigned long long)) == cudaSuccess &&
+                     cudaMalloc(&e->d_trace, 2 * PH_COUNT * sizeof(unsigned long long)) == cudaSuccess &&
+                     cudaMemcpy(e->d_mems, hm.data(), n * sizeof(Member), cudaMemcpyHostToDevice) == cudaSuccess &&
+                     cudaMemcpy(e->d_ctls, hc.data(), n * sizeof(Ctl*), cudaMemcpyHostToDevice) == cudaSuccess &&
+                     cudaMemset(e->d_trace, 0, 2 * PH_COUNT * sizeof(unsigned long long)) == cudaSuccess;
+    if (!okk) return false;
+    a.mems = e->d_mems;
+    a.ctls = e->d_ctls;
+    a.nmem = n;
+    a.bar = e->d_bar;
+    a.counter = e->d_counter;
+    a.trace = nullptr;
+    e->grid = nsm * std::min(occ, 2);
+    e->smem = smem;
+    return true;
+}
 
 extern "C" int fi_ensemble_create(fi_handle* const* members, int32_t n, fi_ensemble** out) {
     if (!members || n < 1 || !out) return FI_ERR_ARG;
@@ -1604,6 +1699,11 @@ extern "C" int fi_ensemble_create(fi_handle* const* members, int32_t n, fi_ensem
     e->mem.assign(members, members + n);
     e->ev_start.resize(n);
     e->ev_end.resize(n);
+    e->persist = ensemble_setup_persist(e);
+    if (!e->persist) {
+        ensemble_free(e);
+        cudaGetLastError();
+    }
     for (int i = 0; i < n; i++) {
         // each member's step loop is a CUDA graph (the persistent executor assumes the
         // whole GPU); the members' graphs overlap on their streams
@@ -1625,6 +1725,7 @@ void fi_ensemble_destroy(fi_ensemble* e) {
         if (ev) cudaEventDestroy(ev);
     for (cudaEvent_t ev : e->ev_end)
         if (ev) cudaEventDestroy(ev);
+    ensemble_free(e);
     delete e;
 }
 
@@ -1659,6 +1760,86 @@ static int ensemble_launch_segment(fi_handle* h) {
     return launch_segment_graph_async(h);
 }
 
+// Persistent path of fi_ensemble_step: each launch runs one segment of every member
+// that has one left; members are prepared (FSAL, t_stop) and finished on the host.
+static int ensemble_step_persist(fi_ensemble* e, std::vector<std::vector<double>>& rest, std::vector<int>& st,
+                                 std::vector<int>& state, int32_t* status) {
+    const int n = (int)e->mem.size();
+    double ms_total = 0.0;
+    for (;;) {
+        bool any = false;
+        for (int i = 0; i < n; i++) {
+            if (state[i] != 0) continue;
+            fi_handle* h = e->mem[i];
+            if (h->tstops.empty()) { state[i] = 2; continue; }
+            int rc = FI_OK;
+            if (h->fsal_pending) {
+                rc = reeval_fsal(h);
+                h->fsal_pending = false;
+                if (!rc && h->ctl.status != FI_OK) rc = set_err(h, h->ctl.status, "%s", fi_status_string(h->ctl.status));
+            }
+            if (!rc) rc = read_ctl(h);
+            if (!rc) {
+                h->ctl.t_stop = h->tstops.front();
+                rc = write_ctl(h);
+            }
+            if (rc) { st[i] = rc; state[i] = 2; continue; }
+            state[i] = 1;
+            any = true;
+        }
+        // members without a segment this round must not step: their t_stop is their t
+        for (int i = 0; i < n; i++) {
+            if (state[i] == 1) continue;
+            fi_handle* h = e->mem[i];
+            if (read_ctl(h) == FI_OK) {
+                h->ctl.t_stop = h->ctl.t;
+                write_ctl(h);
+            }
+        }
+        if (!any) break;
+        if (cudaMemsetAsync(e->d_bar, 0, 4 * sizeof(unsigned int), e->stream) != cudaSuccess ||
+            cudaMemsetAsync(e->d_counter, 0, sizeof(unsigned long long), e->stream) != cudaSuccess)
+            return FI_ERR_CUDA;
+        void* args[] = {(void*)&e->args};
+        cudaEventRecord(e->e0, e->stream);
+        cudaError_t ce = cudaLaunchCooperativeKernel((const void*)k_ens, dim3(e->grid), dim3(ROW_THREADS), args,
+                                                     e->smem, e->stream);
+        cudaEventRecord(e->e1, e->stream);
+        unsigned int bar[4] = {0, 0, 0, 0};
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(bar, e->d_bar, sizeof(bar), cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+        if (ce != cudaSuccess) {
+            for (int i = 0; i < n; i++)
+                if (state[i] == 1) {
+                    st[i] = set_err(e->mem[i], FI_ERR_CUDA, "ensemble kernel: %s", cudaGetErrorString(ce));
+                    state[i] = 2;
+                }
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e->e0, e->e1);
+        ms_total += ms;
+        e->launches += 1;
+        for (int i = 0; i < n; i++) {
+            if (state[i] != 1) continue;
+            fi_handle* h = e->mem[i];
+            const int rc = bar[2] ? set_err(h, FI_ERR_TIMEOUT, "ensemble kernel: a grid barrier wait gave up")
+                                  : ensemble_finish_segment(h);
+            state[i] = rc ? 2 : 0;
+            if (rc) st[i] = rc;
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        fi_handle* h = e->mem[i];
+        h->tstops.insert(h->tstops.end(), rest[i].begin(), rest[i].end());
+        h->last_call = 0;
+    }
+    e->last_gpu_ms = ms_total;
+    if (status)
+        for (int i = 0; i < n; i++) status[i] = st[i];
+    return FI_OK;
+}
+
 extern "C" int fi_ensemble_step(fi_ensemble* e, double dt, int32_t* status) {
     if (!e || !(dt > 0)) return FI_ERR_ARG;
     const int n = (int)e->mem.size();
@@ -1677,6 +1858,7 @@ extern "C" int fi_ensemble_step(fi_ensemble* e, double dt, int32_t* status) {
         while (!v.empty() && v.back() > next_t) { rest[i].insert(rest[i].begin(), v.back()); v.pop_back(); }
         if (cudaEventRecord(e->ev_start[i], h->stream) != cudaSuccess) { st[i] = FI_ERR_CUDA; state[i] = 2; }
     }
+    if (e->persist) return ensemble_step_persist(e, rest, st, state, status);
     for (;;) {
         bool any = false;
         for (int i = 0; i < n; i++) {
@@ -1719,6 +1901,26 @@ extern "C" int fi_ensemble_step(fi_ensemble* e, double dt, int32_t* status) {
 }
 
 extern "C" double fi_ensemble_last_gpu_ms(const fi_ensemble* e) { return e ? e->last_gpu_ms : 0.0; }
+
+extern "C" int fi_ensemble_trace(fi_ensemble* e, int32_t on, double* ms, int64_t* counts) {
+    if (!e) return FI_ERR_ARG;
+    if (!e->persist) return FI_ERR_UNSUPPORTED;
+    cudaSetDevice(e->mem[0]->cfg.device);
+    if (ms && counts) {
+        unsigned long long v[2 * PH_COUNT];
+        if (cudaMemcpy(v, e->d_trace, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return FI_ERR_CUDA;
+        for (int p = 0; p < PH_COUNT; p++) {
+            ms[p] = (double)v[2 * p] * 1e-6;
+            counts[p] = (int64_t)v[2 * p + 1];
+        }
+    }
+    if (on >= 0) {
+        if (on && cudaMemset(e->d_trace, 0, 2 * PH_COUNT * sizeof(unsigned long long)) != cudaSuccess)
+            return FI_ERR_CUDA;
+        e->args.trace = on ? e->d_trace : nullptr;
+    }
+    return FI_OK;
+}
 
 extern "C" int fi_get_stats(fi_handle* h, fi_stats* st) {
     if (h) cudaSetDevice(h->cfg.device);

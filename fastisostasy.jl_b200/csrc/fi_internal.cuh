@@ -91,6 +91,8 @@ struct Member {
     double dt_sparse;
     float zbss_scalar;
     int ncols;                  // column tasks (corner partials per right-hand side)
+    int h_rows, B_cols, h_conv, B_conv;        // tile height / width of each phase
+    int n_rows, n_crow, n_ccol, n_crowi;       // task counts (n_cols == ncols)
     FwdLayout fl;               // forward row phase staging layout
     // state
     double* u[2];               // FP64 state double buffer

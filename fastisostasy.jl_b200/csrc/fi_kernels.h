@@ -53,6 +53,22 @@ __global__ void k_persist(PersistArgs a);
 size_t persist_layout(int nx, int ny, int Mx, int My, int K, int fwd_bytes, int h_rows, int ncols, int B_cols,
                       int h_conv, int B_conv, PersistArgs* a);
 
+// ---- persistent ensemble executor (fi_ensemble.cu) ----
+constexpr int ENS_MAX_MEMBERS = 256;
+struct EnsArgs {
+    const Member* mems;          // member descriptors (device)
+    Ctl* const* ctls;            // their control blocks (device array of pointers)
+    int nmem;
+    unsigned int* bar;           // grid barrier words
+    unsigned long long* counter; // task counter, monotonic within a launch
+    int ws_bytes;                // phase workspace
+    int tw_cap;                  // float2 slots of the staged twiddle table
+    int tice_cap;                // doubles of the staged ice-time table
+    unsigned long long* trace;   // optional phase timeline
+};
+__global__ void k_ens(EnsArgs a);
+size_t ens_layout(const Member* host_mems, int n, EnsArgs* a);
+
 // ---- FP64 transforms and set-up (fi_setup.cu) ----
 __global__ void k_fft64_rows(double2* a, int nx, int ny, int pitch, const FftPlan* plans, int plan, int inverse,
                              int rows_per_block);

@@ -19,88 +19,11 @@
 // the four transform plans with their twiddles and the ice-time table are staged in
 // shared memory once per launch.
 //
-// The grid barrier is an arrival counter plus a generation word.  Each wait is
-// bounded: after PERSIST_SPIN_LIMIT polls the block raises the abort word and leaves,
-// every other block sees the abort word at its next poll and leaves too, and the
-// host reports FI_ERR_TIMEOUT.  A cooperative launch guarantees that all blocks are
-// resident, so the bound is only reached if the launch is broken.
-#include "fi_phases.cuh"
+// The grid barrier, the phase timeline marks and the warp-level controller are in
+// fi_grid.cuh.
+#include "fi_grid.cuh"
 
 namespace fi {
-
-constexpr long long PERSIST_SPIN_LIMIT = 1LL << 24;  // polls of >= 64 ns each, about 1 s or more
-
-// Returns false (in every thread of the block) when the barrier was abandoned.
-__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, int* s_ok) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = bar + 1;
-        volatile unsigned int* vabort = bar + 2;
-        const unsigned int gen = *vgen;
-        int ok = 1;
-        __threadfence();
-        const unsigned int prev = atomicAdd(bar, 1u);
-        if (prev == nblocks - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            long long polls = 0;
-            while (*vgen == gen) {
-                if (*vabort) { ok = 0; break; }
-                if (++polls > PERSIST_SPIN_LIMIT) {
-                    atomicExch(bar + 2, 1u);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        *s_ok = ok;
-    }
-    __syncthreads();
-    return *s_ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-
-// phase timeline (block 0, thread 0): time since the previous mark goes to phase ph
-__device__ __forceinline__ void trace_mark(unsigned long long* trace, unsigned long long* last, int ph) {
-    if (trace && blockIdx.x == 0 && threadIdx.x == 0) {
-        const unsigned long long now = globaltimer_ns();
-        trace[2 * ph] += now - *last;
-        trace[2 * ph + 1] += 1;
-        *last = now;
-    }
-}
-
-// loop footer + header of the next attempt (finish_attempt of the per-phase kernels),
-// run by the first warp: lanes 0 and 1 evaluate the controller's two powers side by side
-__device__ inline void persist_finish_attempt(const Member& m, Ctl* c, double EEst) {
-    const int lane = threadIdx.x & 31;
-    const double base = lane == 0 ? EEst : c->qold;
-    const double ex = lane == 0 ? PI_BETA1 : PI_BETA2;
-    const bool pw = (EEst == EEst) && EEst != 0.0;
-    const double pv = (pw && lane < 2) ? pow(base, ex) : 1.0;
-    const double qold_b2 = __shfl_sync(0xffffffffu, pv, 1);
-    if (lane != 0) return;
-    controller_update_pw(c, EEst, pw ? pv : 0.0, pw ? qold_b2 : 1.0, m.tout);
-    int active = (c->status == FI_OK);
-    c->nsteps_seg += 1;
-    if (c->accept_step && (c->pending_output || !(c->t < c->t_stop))) active = 0;
-    if (active) {
-        loopheader_prep(c);
-        if (c->status != FI_OK) active = 0;
-    }
-    c->active = active;
-    c->gate = 0;
-    if (active) gate_eval(m, c, c->t + C2 * c->dt);
-}
 
 __global__ void __launch_bounds__(RT, 2) k_persist(PersistArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -270,7 +193,7 @@ __global__ void __launch_bounds__(RT, 2) k_persist(PersistArgs a) {
         // ---- step controller, replicated: the partials in a fixed order per lane ----
         if (tid < 32) {
             const double acc = partials_sum(m.partial, a.n_rows);
-            persist_finish_attempt(m, &sc, sqrt(acc / ((double)nx * ny)));
+            finish_attempt_warp(m, &sc, sqrt(acc / ((double)nx * ny)));
         }
         __syncthreads();
         if (tid < 4 && sc.active) s_uc[tid] = __ldcg(&m.u[sc.ibuf][corner_index(tid, nx, ny)]);

@@ -372,10 +372,13 @@ class Simulation:
     dz_ss_ref, z_b_ref, nout, c) -- src/simulation.jl:105-156.
 
     ``form`` picks the compute form: "fp32" (fused FP32 kernels with FP64 state,
-    the default) or "fp64" (the plain FP64 form)."""
+    the default) or "fp64" (the plain FP64 form).  ``tiles`` = (rows per row task,
+    spectral columns per column task) of the FP32 kernels; None takes the tuned value
+    for square grids from fastiso_b200.autotune's table, else the library's default."""
 
     def __init__(self, domain, bcs, sealevel, solidearth, t_span, *, opts=None, u_ref=None, ue_ref=None,
-                 dz_ss_ref=None, z_b_ref=None, nout=None, c=None, form="fp32", max_steps=1_000_000, device=0):
+                 dz_ss_ref=None, z_b_ref=None, nout=None, c=None, form="fp32", max_steps=1_000_000, device=0,
+                 tiles=None):
         self.domain, self.bcs, self.sealevel, self.solidearth = domain, bcs, sealevel, solidearth
         self.opts = opts or SolverOptions()
         self.c = c or PhysicalConstants()
@@ -428,6 +431,7 @@ class Simulation:
         cfg.device = int(device)
         self.form = form
         self.cfg = cfg
+        self.tiles = tiles
         self.elastic_table = get_greenintegrand_coeffs()
         self._handle = None
         self._initialized = False
@@ -473,6 +477,12 @@ class Simulation:
         if rc != abi.FI_OK:
             raise abi.FiError(rc, "fi_create failed")
         self._handle = h
+        if self.tiles is None and self.cfg.form == abi.FI_FORM_FP32 and self.domain.nx == self.domain.ny:
+            from .autotune import tiles_for  # noqa: WPS433 (the tuner imports this module)
+
+            self.tiles = tiles_for(f"single:{self.domain.nx}")
+        if self.tiles is not None and self.cfg.form == abi.FI_FORM_FP32:
+            self._check(lib.fi_set_tiles(h, int(self.tiles[0]), int(self.tiles[1])), "fi_set_tiles")
         inp = self.prepared_inputs()
         for name, arr in inp["fields"].items():
             self.set_field(name, arr)
@@ -605,14 +615,24 @@ class Ensemble:
     every member, the members' step loops running concurrently on the GPU.  A member
     that fails is reported in the returned status list and does not stop the others."""
 
-    def __init__(self, sims):
+    #: tile shape of members whose handles do not exist yet when the tuning table has
+    #: no entry: tall tiles, since the ensemble is throughput-bound
+    DEFAULT_TILES = (8, 8)
+
+    def __init__(self, sims, tiles="auto"):
         self.sims = list(sims)
         if not self.sims:
             raise ValueError("an ensemble needs at least one member")
+        if isinstance(tiles, str):
+            from .autotune import tiles_for  # noqa: WPS433
+
+            tiles = tiles_for(f"ensemble:{len(self.sims)}") or self.DEFAULT_TILES
         self.integrators = []
         for s in self.sims:
             if s.cfg.form != abi.FI_FORM_FP32:
                 raise UnsupportedError("ensemble members use the FP32 form")
+            if s._handle is None and s.tiles is None and tiles is not None:
+                s.tiles = tuple(tiles)
             self.integrators.append(init_integrator(s))
         self.lib = self.sims[0].lib
         arr = (C.c_void_p * len(self.sims))(*[s._handle.value for s in self.sims])
@@ -632,6 +652,16 @@ class Ensemble:
     @property
     def last_gpu_ms(self):
         return float(self.lib.fi_ensemble_last_gpu_ms(self._h))
+
+    def trace(self, on=None):
+        """Phase timeline of the persistent ensemble executor: ``trace(True)`` starts
+        recording, ``trace()`` returns {phase: (ms, count)}, ``trace(False)`` stops."""
+        ms = (C.c_double * abi.FI_NUM_PHASES)()
+        cnt = (C.c_int64 * abi.FI_NUM_PHASES)()
+        rc = self.lib.fi_ensemble_trace(self._h, -1 if on is None else int(bool(on)), ms, cnt)
+        if rc != abi.FI_OK:
+            raise abi.FiError(rc, "fi_ensemble_trace failed")
+        return {name: (m, c) for name, m, c in zip(abi.PHASE_NAMES, ms, cnt)}
 
     def close(self):
         if getattr(self, "_h", None):

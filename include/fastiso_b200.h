@@ -173,6 +173,14 @@ int fi_set_elastic_table(fi_handle* h, int32_t n, const double* rm, const double
 int fi_set_channel_scaling(fi_handle* h, int32_t n, const double* visc_ratio_mean,
                            const double* channel_thickness_mean);
 
+/* No counterpart in the reference: tile shape of the FP32 kernels, between fi_create
+ * and fi_init.  h_rows: rows per row task (row FFTs, stencils), B_cols: spectral
+ * columns per column task, both in [1, 16].  Small tiles favour a single simulation
+ * (latency), tall tiles an ensemble (throughput); fastiso_b200.autotune measures them.
+ * Results agree to FP32 rounding across tile shapes (the row FFTs pair halo rows
+ * differently). */
+int fi_set_tiles(fi_handle* h, int32_t h_rows, int32_t B_cols);
+
 /* Reference state + init_problem! (src/simulation.jl:129-156, 305-312): builds the
  * Green's functions and spectral factors, the reference state, and performs the
  * first RHS evaluation (which forces the sparse update). */
@@ -243,15 +251,21 @@ int fi_get_phase_trace(fi_handle* h, double* ms, int64_t* counts);
  * host-threaded ensemble of ext/FastIsostasyEnsembleKalmanProcessesExt.jl:107-122).
  * An ensemble groups initialised FP32 handles on one device, each with its own grid,
  * fields, tolerances and integrator (fi_init_integrator called).  fi_ensemble_step(e,
- * dt, status) is step!(integrator_m, dt, true) for every member m, with the members'
- * step loops running concurrently on their streams; status[m] (n entries, may be NULL)
- * receives each member's FI_* code, and a failing member does not stop the others.
+ * dt, status) is step!(integrator_m, dt, true) for every member m, all members
+ * advancing together in one persistent cooperative kernel per segment; status[m]
+ * (n entries, may be NULL) receives each member's FI_* code, and a failing member does not stop the others.
  * fi_ensemble_last_gpu_ms: device time of the last fi_ensemble_step (first start to
  * last end over the members' streams).  The ensemble does not own its members. */
 typedef struct fi_ensemble fi_ensemble;
 int fi_ensemble_create(fi_handle* const* members, int32_t n, fi_ensemble** out);
 int fi_ensemble_step(fi_ensemble* e, double dt, int32_t* status);
 double fi_ensemble_last_gpu_ms(const fi_ensemble* e);
+/* Phase timeline of the persistent ensemble executor (FI_ERR_UNSUPPORTED for the
+ * stream executor): on = 1 clears and starts recording, 0 stops, -1 leaves it; ms and
+ * counts (FI_NUM_PHASES each, may be NULL) receive the sums as fi_get_phase_trace.
+ * FI_ENS_EXECUTOR=streams (read by fi_ensemble_create) selects the stream executor:
+ * one CUDA graph per member on its own stream. */
+int fi_ensemble_trace(fi_ensemble* e, int32_t on, double* ms, int64_t* counts);
 void fi_ensemble_destroy(fi_ensemble* e);
 
 const char* fi_last_error(const fi_handle* h);

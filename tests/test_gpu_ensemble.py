@@ -1,5 +1,6 @@
 """Batched ensembles (fi_ensemble_*): members of different grids stepped together give
-bitwise the results of stepping each member alone, and a failing member is flagged
+bitwise the results of stepping each member alone (with the persistent ensemble kernel
+and with one CUDA graph per member on its own stream), and a failing member is flagged
 without stopping the others."""
 import numpy as np
 import pytest
@@ -11,7 +12,10 @@ from helpers import F_, RUN_TOL, oracle_for, rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def member(N, mean_log10eta, seed, t_end=400.0, t_ice_end=None):
+TILES = F.Ensemble.DEFAULT_TILES
+
+
+def member(N, mean_log10eta, seed, t_end=400.0, t_ice_end=None, tiles=TILES):
     W_ = 15e3 * N
     domain = F.RegionalDomain(W_, W_, N, N)
     rng = np.random.default_rng(seed)
@@ -22,13 +26,15 @@ def member(N, mean_log10eta, seed, t_end=400.0, t_ice_end=None):
     it = F.TimeInterpolatedIceThickness([0.0, 1.0, te], [domain.zeros(), H1, 1.2 * H1], domain)
     bcs = F.BoundaryConditions(domain, ice_thickness=it)
     sl = F.RegionalSeaLevel(surface=F.LaterallyVariableSeaSurface())
-    return F.Simulation(domain, bcs, sl, se, (0.0, t_end), form="fp32")
+    return F.Simulation(domain, bcs, sl, se, (0.0, t_end), form="fp32", tiles=tiles)
 
 
 SPECS = [(32, 21.0, 1), (48, 20.5, 2), (40, 21.5, 3)]
 
 
-def test_ensemble_bitwise_equals_members_alone():
+@pytest.mark.parametrize("executor", ["persist", "streams"])
+def test_ensemble_bitwise_equals_members_alone(monkeypatch, executor):
+    monkeypatch.setenv("FI_ENS_EXECUTOR", executor)
     alone = []
     for N, mu, seed in SPECS:
         sim = member(N, mu, seed)
@@ -38,7 +44,7 @@ def test_ensemble_bitwise_equals_members_alone():
         alone.append((F_(sim.get_field("u")), F_(sim.get_field("ue")), sim.stats()))
         sim.close()
     sims = [member(N, mu, seed) for N, mu, seed in SPECS]
-    ens = F.Ensemble(sims)
+    ens = F.Ensemble(sims, tiles=TILES)
     assert ens.step(150.0) == [abi.FI_OK] * len(SPECS)
     assert ens.step(150.0) == [abi.FI_OK] * len(SPECS)
     assert ens.last_gpu_ms > 0
@@ -58,7 +64,7 @@ def test_ensemble_member_parity_with_oracle():
     sim.nout.t = [300.0]
     ref = oracle_for(sim)
     ref.init()
-    ens = F.Ensemble([sim, member(32, 21.0, 7)])
+    ens = F.Ensemble([sim, member(32, 21.0, 7)], tiles=TILES)
     ref.init_integrator(np.asarray([300.0]))
     ens.step(300.0)
     ref.step(300.0)
@@ -69,7 +75,7 @@ def test_ensemble_failing_member_is_isolated():
     # the middle member's ice history ends at 200 yr: stepping to 300 yr leaves its
     # forcing range (TimeInterpolation2D out of range); the others are unaffected
     sims = [member(32, 21.0, 1), member(48, 20.5, 2, t_ice_end=200.0), member(40, 21.5, 3)]
-    ens = F.Ensemble(sims)
+    ens = F.Ensemble(sims, tiles=TILES)
     st = ens.step(300.0)
     assert st[0] == abi.FI_OK and st[2] == abi.FI_OK
     assert st[1] == abi.FI_ERR_FORCING_RANGE

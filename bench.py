@@ -213,28 +213,21 @@ ENS_MEMBERS = 128
 ENS_WINDOW_YR = 1000.0
 
 
-def ensemble_bench(dev):
+def ensemble_bench(dev, rank=0, world=1):
     """Config 3: 128 members, N drawn from {64, 96, 128, 192, 256} over N x 30 km, own
     seeded viscosity fields, shared disc + random-field ice history; the persistent
-    ensemble executor advances all members one window; against looping the plain FP64
-    form member by member (sampled on 4 members)."""
+    ensemble executor advances all members one window.  Under torchrun the members are
+    sharded over the ranks (greedy bin-packing on N^2 log N, no communication in the time
+    loop, one gather at the end) and the window's time is the slowest rank's.  Compared
+    against looping the plain FP64 form member by member (sampled on 4 members, rank 0)."""
+    from fastiso_b200.shard import run_shard
+
     members, t_ice, mod = W.config3_members(n_members=ENS_MEMBERS)
-    sims = [W.config3_simulation(m, t_ice, mod, form="fp32") for m in members]
-    for sm in sims:
-        sm.cfg.device = dev
-        sm.cfg.max_steps = 50_000_000
-    ens = F.Ensemble(sims)
-    ens.step(50.0)
-    c0 = [sm.stats() for sm in sims]
-    st = ens.step(ENS_WINDOW_YR)
-    ms = ens.last_gpu_ms
-    c1 = [sm.stats() for sm in sims]
-    steps = [(b["naccept"] + b["nreject"]) - (a["naccept"] + a["nreject"]) for a, b in zip(c0, c1)]
-    rhs = sum(b["nf"] - a["nf"] for a, b in zip(c0, c1))
-    tiles = list(sims[0].tiles) if sims[0].tiles else None
-    ens.close()
-    for sm in sims:
-        sm.close()
+    parts = run_shard(members, t_ice, mod, ENS_WINDOW_YR, rank, world, device=dev)
+    if rank != 0:
+        return None
+    ms = max(p["ms"] for p in parts)
+    ok = all(x == 0 for p in parts for x in p["status"])
     tot_kyr, tot_ms = 0.0, 0.0
     for m in members[:4]:
         ps = W.config3_simulation(m, t_ice, mod, form="fp64")
@@ -248,11 +241,13 @@ def ensemble_bench(dev):
         ps.close()
     v = ENS_MEMBERS * ENS_WINDOW_YR / 1e3 / (ms / 1e3)
     plain = tot_kyr / (tot_ms / 1e3)
-    return {"value": v, "unit": "member-kyr/s", "members": ENS_MEMBERS,
+    from fastiso_b200.autotune import tiles_for
+
+    return {"value": v, "unit": "member-kyr/s", "members": ENS_MEMBERS, "ranks": world,
+            "members_per_rank": [len(p["members"]) for p in parts],
             "window": f"{ENS_WINDOW_YR:g} yr after 50 yr (of config 3's 20 kyr)",
-            "tiles": tiles, "status_ok": all(x == 0 for x in st),
-            "steps_per_member": {"min": min(steps), "mean": sum(steps) / len(steps), "max": max(steps)},
-            "rhs_evals_per_s": rhs / (ms / 1e3),
+            "tiles": list(tiles_for(f"ensemble:{len(parts[0]['members'])}") or F.Ensemble.DEFAULT_TILES),
+            "status_ok": ok, "ms": ms,
             "plain_fp64_loop": {"value": plain, "unit": "member-kyr/s",
                                 "sample": "4 members x 200 yr after 50 yr, one after another"},
             "speedup_vs_plain_loop": v / plain}
@@ -336,6 +331,8 @@ def run_gpu(args, rank, world, dev):
             torch.distributed.barrier()
     c1 = counters(sim)
     phases = phase_timeline(sim, integ) if rank == 0 else None
+    sim.close()
+    ens = ensemble_bench(dev, rank, world)
     t_total = float(sum(step_ms))
     if world > 1:
         tt = torch.tensor([t_total], dtype=torch.float64, device=f"cuda:{dev}")
@@ -345,7 +342,6 @@ def run_gpu(args, rank, world, dev):
     value = world * kyr / (t_total / 1e3)
     attempts = (c1["naccept"] + c1["nreject"]) - (c0["naccept"] + c0["nreject"])
     launches = launches_between(c0, c1, c1["executor"])
-    sim.close()
     if rank != 0:
         return
     # ---- e2e: coupling API with host buffers -------------------------------------
@@ -388,8 +384,6 @@ def run_gpu(args, rank, world, dev):
     # ---- roofline of the dominant kernel ----------------------------------------
     seg = max(1, c1["segments"] - c0["segments"])
     roof = roofline(dev, 1e3 * t_total / max(1, attempts), attempts / seg, c1["executor"], c1["grid"])
-    # ---- batched ensemble (config 3) ----------------------------------------------
-    ens = ensemble_bench(dev)
     # ---- CPU baseline (oracle) ---------------------------------------------------
     cpu_v, cores, yrs = cpu_oracle_sample()
     line = {
@@ -429,6 +423,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fused", choices=["fused", "reference"])
+    ap.add_argument("--profile-ensemble", action="store_true",
+                    help="small config-3 ensemble (16 members, 20 yr) for an ncu capture of k_ens")
     ap.add_argument("--profile", action="store_true",
                     help="only a short fused N=350 segment (10 yr warm-up + 5 yr) for ncu captures")
     args = ap.parse_args()
@@ -445,6 +441,17 @@ def main():
         import datetime
 
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.profile_ensemble:
+        members, t_ice, mod = W.config3_members(n_members=16)
+        sims = [W.config3_simulation(m, t_ice, mod, form="fp32") for m in members]
+        for sm in sims:
+            sm.cfg.device = local
+        ens = F.Ensemble(sims)
+        ens.step(20.0)
+        print(json.dumps({"profile_case": "config3 16 members, 20 yr", "ms": ens.last_gpu_ms,
+                          "steps": [sm.stats()["naccept"] + sm.stats()["nreject"] for sm in sims]}))
+        ens.close()
+        return
     if args.profile:
         sim = W.config2(form="fp32", N=N350)
         sim.cfg.device = local

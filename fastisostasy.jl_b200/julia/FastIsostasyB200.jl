@@ -1,0 +1,145 @@
+# FastIsostasyB200.jl -- Julia `ccall` shim over libfastiso_b200.so (include/fastiso_b200.h).
+#
+# Builds a B200 handle from a FastIsostasy `Simulation` (the reference's own constructors
+# prepare every input: rigidity, effective viscosity, R, masks, reference state, ice
+# history) and runs `run!` / `init_integrator` + `step!` semantics on the GPU.  Julia
+# matrices are column-major with dimension 1 = x, which is the C ABI's layout, so arrays
+# are passed without a transpose.  Not exercised here: this build environment has no Julia.
+module FastIsostasyB200
+
+using FastIsostasy
+
+const LIB = get(ENV, "FASTISO_B200_LIB", joinpath(@__DIR__, "..", "lib", "libfastiso_b200.so"))
+
+const FI_FORM_FP32 = Int32(0)
+const FI_FORM_FP64 = Int32(1)
+
+# field ids (fi_set_field / fi_get_field)
+const F = (litho_rigidity = 0, effective_viscosity = 1, pseudodiff_scaling = 2, maskactive = 3,
+           u_ref = 4, ue_ref = 5, dz_ss_ref = 6, z_b_ref = 7, u = 8, ue = 9, dudt = 10, dz_ss = 11,
+           H_ice = 12, z_ss = 13, z_b = 14)
+
+# fi_config, field for field (isbits: Julia lays it out as C does)
+mutable struct FiConfig
+    nx::Int32; ny::Int32
+    Wx::Float64; Wy::Float64
+    mE::Float64; r_pole::Float64; g::Float64; seconds_per_year::Float64
+    rho_ice::Float64; rho_water::Float64; rho_seawater::Float64
+    rho_litho::Float64; rho_uppermantle::Float64; litho_poissonratio::Float64
+    lithosphere::Int32; lithosphere_column::Int32; sea_surface::Int32
+    z_bsl::Float64
+    bc_viscous_border::Float64; bc_elastic_border::Float64; bc_sea_surface_border::Float64
+    ice_mode::Int32; ice_flat_bc::Int32
+    t0::Float64; t1::Float64; reltol::Float64; abstol::Float64; dt_sparse_diagnostics::Float64
+    max_steps::Int64
+    form::Int32; device::Int32
+end
+
+FiConfig() = FiConfig(zeros(Int32, 2)..., zeros(12)..., zeros(Int32, 3)..., zeros(4)..., zeros(Int32, 2)...,
+                      zeros(5)..., Int64(0), Int32(0), Int32(0))
+
+mutable struct B200Simulation
+    sim::Any
+    h::Ptr{Cvoid}
+end
+
+function check(rc::Cint, h::Ptr{Cvoid}, what)
+    rc == 0 && return nothing
+    msg = h == C_NULL ? "" : unsafe_string(ccall((:fi_last_error, LIB), Cstring, (Ptr{Cvoid},), h))
+    error("$what failed ($rc): $msg")
+end
+
+set_field!(b::B200Simulation, id::Integer, X::AbstractMatrix) =
+    check(ccall((:fi_set_field, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Csize_t),
+                b.h, id, Array{Float64}(X), length(X)), b.h, "fi_set_field")
+
+function getfield_b200(b::B200Simulation, id::Integer)
+    d = b.sim.domain
+    X = Matrix{Float64}(undef, d.nx, d.ny)
+    check(ccall((:fi_get_field, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Csize_t), b.h, id, X, length(X)),
+          b.h, "fi_get_field")
+    return X
+end
+
+"""
+    B200Simulation(sim, t_span; form = :fp32, device = 0)
+
+A GPU twin of `sim` (laterally-variable ELVA with Maxwell mantle) over `t_span`, the
+same tuple given to `Simulation`: the same inputs, run by libfastiso_b200.so.
+"""
+function B200Simulation(sim, t_span; form = :fp32, device = 0)
+    d, c, se, sl, bcs = sim.domain, sim.c, sim.solidearth, sim.sealevel, sim.bcs
+    cfg = FiConfig()
+    ccall((:fi_config_default, LIB), Cvoid, (Ref{FiConfig}, Int32, Int32, Float64, Float64), cfg, d.nx, d.ny,
+          d.Wx, d.Wy)
+    cfg.mE, cfg.r_pole, cfg.g, cfg.seconds_per_year = c.mE, c.r_pole, c.g, c.seconds_per_year
+    cfg.rho_ice, cfg.rho_water, cfg.rho_seawater = c.rho_ice, c.rho_water, c.rho_seawater
+    cfg.rho_litho, cfg.rho_uppermantle = se.rho_litho, se.rho_uppermantle
+    cfg.litho_poissonratio = se.litho_poissonratio
+    cfg.lithosphere = se.lithosphere isa RigidLithosphere ? Int32(1) : Int32(0)
+    cfg.lithosphere_column = se.lithosphere_column isa CompressibleLithosphereColumn ? Int32(1) : Int32(0)
+    cfg.sea_surface = sl.surface isa LaterallyVariableSeaSurface ? Int32(1) : Int32(0)
+    cfg.bc_viscous_border = bcs.viscous_displacement.x_border
+    cfg.bc_elastic_border = bcs.elastic_displacement.x_border
+    cfg.bc_sea_surface_border = bcs.sea_surface_perturbation.x_border
+    it = bcs.ice_thickness
+    timeinterp = it isa TimeInterpolatedIceThickness
+    cfg.ice_mode = timeinterp ? Int32(0) : Int32(1)
+    cfg.t0, cfg.t1 = Float64(t_span[1]), Float64(t_span[2])
+    cfg.form = form == :fp32 ? FI_FORM_FP32 : FI_FORM_FP64
+    cfg.device = device
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:fi_create, LIB), Cint, (Ref{FiConfig}, Ref{Ptr{Cvoid}}), cfg, h), C_NULL, "fi_create")
+    b = B200Simulation(sim, h[])
+    finalizer(x -> ccall((:fi_destroy, LIB), Cvoid, (Ptr{Cvoid},), x.h), b)
+    set_field!(b, F.litho_rigidity, se.litho_rigidity)
+    set_field!(b, F.effective_viscosity, se.effective_viscosity)
+    set_field!(b, F.pseudodiff_scaling, se.pseudodiff_scaling)
+    set_field!(b, F.maskactive, Float64.(se.maskactive))
+    set_field!(b, F.u_ref, sim.ref.u)
+    set_field!(b, F.ue_ref, sim.ref.ue)
+    set_field!(b, F.z_b_ref, sim.ref.z_b)
+    if timeinterp
+        t = Vector{Float64}(it.t_vec)
+        H = cat((Array{Float64}(X) for X in it.H_vec)...; dims = 3)
+        check(ccall((:fi_set_ice_history, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}),
+                    b.h, length(t), t, H), b.h, "fi_set_ice_history")
+    end
+    rm, GE = FastIsostasy.get_greenintegrand_coeffs(Float64)
+    check(ccall((:fi_set_elastic_table, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}),
+                b.h, length(rm), Vector{Float64}(rm), Vector{Float64}(GE)), b.h, "fi_set_elastic_table")
+    check(ccall((:fi_init, LIB), Cint, (Ptr{Cvoid},), b.h), b.h, "fi_init")
+    return b
+end
+
+"""run!(b): integrate t_span and fill b.sim.nout with u, ue, dudt and dz_ss at nout.t."""
+function run!(b::B200Simulation)
+    tout = Vector{Float64}(b.sim.nout.t)
+    d = b.sim.domain
+    n, k = d.nx * d.ny, length(tout)
+    ot = zeros(k); U = zeros(n * k); UE = zeros(n * k); DU = zeros(n * k); DZ = zeros(n * k)
+    check(ccall((:fi_run, LIB), Cint,
+                (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                b.h, k, tout, ot, U, UE, DU, DZ), b.h, "fi_run")
+    sl(A, i) = reshape(A[(i - 1) * n + 1:i * n], d.nx, d.ny)
+    return (t = ot, u = [sl(U, i) for i in 1:k], ue = [sl(UE, i) for i in 1:k],
+            dudt = [sl(DU, i) for i in 1:k], dz_ss = [sl(DZ, i) for i in 1:k])
+end
+
+"""init_integrator(b) and step!(b, dt): step!(integrator, dt, true) for coupling."""
+function init_integrator(b::B200Simulation)
+    ts = Vector{Float64}(b.sim.nout.t)
+    check(ccall((:fi_init_integrator, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}), b.h, length(ts), ts),
+          b.h, "fi_init_integrator")
+    return b
+end
+
+step!(b::B200Simulation, dt::Real) =
+    check(ccall((:fi_step, LIB), Cint, (Ptr{Cvoid}, Float64), b.h, dt), b.h, "fi_step")
+
+"""Set the ice thickness of an externally updated load (coupling)."""
+set_ice!(b::B200Simulation, H::AbstractMatrix) = set_field!(b, F.H_ice, H)
+
+current_u(b::B200Simulation) = getfield_b200(b, F.u)
+
+end  # module

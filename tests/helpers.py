@@ -33,3 +33,32 @@ RUN_TOL = {"fp64": 1e-6, "fp32": 2e-3}
 #: sparse diagnostics (ue, dz_ss) are sampled at stage times every 10 yr and are more
 #: sensitive to the step sequence
 RUN_TOL_SPARSE = {"fp64": 2e-3, "fp32": 5e-3}
+
+
+# ---- cases of the committed golden fixtures (tests/golden/make_golden.py) ----------
+def golden_sim(form, nx=24, ny=20, t_end=600.0, seed=11):
+    """A small LV-ELVA case with every channel on (elastic, viscous, sea surface),
+    seeded viscosity and lithosphere maps and a ramped disc load."""
+    W_ = 0.6e6
+    domain = F.RegionalDomain(W_, W_ * ny / nx, nx, ny)
+    rng = np.random.default_rng(seed)
+    log10eta = 21 + 0.4 * np.exp(-domain.R**2 / (2 * (W_ / 3) ** 2)) + 0.1 * rng.standard_normal((nx, ny))
+    T = 90e3 + 30e3 * rng.random((nx, ny))
+    se = F.SolidEarth(domain, layer_boundaries=T.reshape(nx, ny, 1),
+                      layer_viscosities=(10**log10eta).reshape(nx, ny, 1))
+    H1 = 1.2e3 * (domain.R < 0.45 * W_)
+    it = F.TimeInterpolatedIceThickness([0.0, 1.0, t_end], [domain.zeros(), H1, 1.1 * H1], domain)
+    bcs = F.BoundaryConditions(domain, ice_thickness=it)
+    sl = F.RegionalSeaLevel(surface=F.LaterallyVariableSeaSurface())
+    return F.Simulation(domain, bcs, sl, se, (0.0, t_end), form=form)
+
+
+def golden_u(sim, seed=12):
+    rng = np.random.default_rng(seed)
+    d = sim.domain
+    return -40 * np.exp(-d.R**2 / (2 * (0.35 * d.Wx) ** 2)) + 0.3 * rng.standard_normal((d.nx, d.ny))
+
+
+GOLDEN_RHS_TIMES = (0.5, 12.5)
+GOLDEN_RUN_TIMES = (300.0, 600.0, 1000.0)
+GOLDEN_RUN_T_END = 1000.0

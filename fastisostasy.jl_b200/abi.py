@@ -219,6 +219,8 @@ _SIGS = {
     "fi_ensemble_last_gpu_ms": (C.c_double, [C.c_void_p]),
     "fi_ensemble_trace": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "fi_ensemble_destroy": (None, [C.c_void_p]),
+    "fi_fno_gemm": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
+                             C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int64]),
     "fi_last_error": (C.c_char_p, [C.c_void_p]),
     "fi_status_string": (C.c_char_p, [C.c_int32]),
     "fi_destroy": (None, [C.c_void_p]),

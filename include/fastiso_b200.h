@@ -268,6 +268,16 @@ double fi_ensemble_last_gpu_ms(const fi_ensemble* e);
 int fi_ensemble_trace(fi_ensemble* e, int32_t on, double* ms, int64_t* counts);
 void fi_ensemble_destroy(fi_ensemble* e);
 
+/* ---- Fourier-neural-operator surrogate (no counterpart in the reference) ----
+ * fi_fno_gemm: C[z] = A[z] * B[z]^T for z < batch on the 5th-generation tensor cores
+ * (tcgen05, BF16 inputs, FP32 accumulation in tensor memory), the channel-mixing and
+ * truncated-DFT kernel of the surrogate, exposed for testing.  Device pointers; A is
+ * M x K and B is N x K with K-contiguous rows (pitches lda, ldb, elements), C is M x N
+ * FP32 (pitch ldc); sA, sB, sC are batch strides in elements.  K, lda, ldb, sA, sB must
+ * be multiples of 8 and A, B 16-byte aligned (FI_ERR_ARG otherwise). */
+int fi_fno_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, const void* B, int32_t ldb,
+                float* C, int32_t ldc, int32_t batch, int64_t sA, int64_t sB, int64_t sC);
+
 const char* fi_last_error(const fi_handle* h);
 const char* fi_status_string(int32_t status);
 void fi_destroy(fi_handle* h);

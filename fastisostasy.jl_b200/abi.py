@@ -221,6 +221,19 @@ _SIGS = {
     "fi_ensemble_destroy": (None, [C.c_void_p]),
     "fi_fno_gemm": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
                              C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int64]),
+    "fi_fno_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "fi_fno_num_params": (C.c_int64, [C.c_void_p]),
+    "fi_fno_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "fi_fno_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "fi_fno_get_grads": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "fi_fno_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "fi_fno_backward": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "fi_fno_train_step": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_float,
+                                    C.POINTER(C.c_float)]),
+    "fi_fno_adam": (C.c_int, [C.c_void_p, C.c_float]),
+    "fi_fno_set_adam": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float]),
+    "fi_fno_last_error": (C.c_char_p, [C.c_void_p]),
+    "fi_fno_destroy": (None, [C.c_void_p]),
     "fi_last_error": (C.c_char_p, [C.c_void_p]),
     "fi_status_string": (C.c_char_p, [C.c_int32]),
     "fi_destroy": (None, [C.c_void_p]),

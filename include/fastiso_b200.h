@@ -278,6 +278,30 @@ void fi_ensemble_destroy(fi_ensemble* e);
 int fi_fno_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, const void* B, int32_t ldb,
                 float* C, int32_t ldc, int32_t batch, int64_t sA, int64_t sB, int64_t sC);
 
+/* The surrogate network: input x [B][6][S][S] FP32 (x fastest; the caller's normalised
+ * fields), output y [B][S][S] FP32.  Lift 6 -> 32, four Fourier layers of width 32
+ * keeping kx in [0,16) x ky in {0..15, S-16..S-1} (GELU after the first three),
+ * projection 32 -> 128 (GELU) -> 1.  S is a multiple of 32 in [32, 256]; batches are
+ * 1..max_batch.  All tensors are device pointers; every call returns after its work has
+ * finished.  Parameters are one flat FP32 vector in this order: P[32][6], bP[32]; per
+ * layer: W[512 modes (kx*32 + kyi)][re, im][ci 32][co 32], Wloc[co][ci], bloc[32];
+ * Q1[128][32], b1[128], Q2[128], b2.  seed draws the default initialisation. */
+typedef struct fi_fno fi_fno;
+int fi_fno_create(int32_t S, int32_t max_batch, int32_t device, uint64_t seed, fi_fno** out);
+int64_t fi_fno_num_params(const fi_fno* h);
+int fi_fno_get_params(fi_fno* h, float* out, int64_t n);      /* host buffer of n floats */
+int fi_fno_set_params(fi_fno* h, const float* in, int64_t n); /* also resets Adam's moments */
+int fi_fno_get_grads(fi_fno* h, float* out, int64_t n);
+int fi_fno_forward(fi_fno* h, int32_t B, const float* x, float* y);
+/* gradients of sum(dy * y) for the last fi_fno_forward (same B), overwriting the previous */
+int fi_fno_backward(fi_fno* h, int32_t B, const float* dy);
+/* forward, mean-squared-error loss against target [B][S][S], backward, one Adam step */
+int fi_fno_train_step(fi_fno* h, int32_t B, const float* x, const float* target, float lr, float* loss);
+int fi_fno_adam(fi_fno* h, float lr); /* one Adam step with the current gradients */
+int fi_fno_set_adam(fi_fno* h, float beta1, float beta2, float eps); /* default 0.9, 0.999, 1e-8 */
+const char* fi_fno_last_error(const fi_fno* h);
+void fi_fno_destroy(fi_fno* h);
+
 const char* fi_last_error(const fi_handle* h);
 const char* fi_status_string(int32_t status);
 void fi_destroy(fi_handle* h);

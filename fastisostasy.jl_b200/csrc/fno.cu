@@ -329,24 +329,25 @@ __global__ void __launch_bounds__(256) k_act_bwd(const float* __restrict__ dv, c
     }
 }
 
-// loss gradient: MSE against target (dq = 2 (q - t) / n, loss += (q - t)^2 / n) or a given dy.
+// loss gradient: weighted MSE against target, loss = (1/n) sum_i w_b(i) (q_i - t_i)^2 with
+// per-sample weights w (1 when null), dq = 2 w (q - t) / n; or a given dy.
 // Writes dq (FP32), its BF16 copy into channel 33 of the last activation buffer, and
 // accumulates sum(dq) (gradient of b2).
 __global__ void __launch_bounds__(256) k_loss(const float* __restrict__ q, const float* __restrict__ target,
-                                              const float* __restrict__ dy, int n, int S2, float inv_n, float* dq,
-                                              bf16* vext4, float* loss, float* gb2) {
+                                              const float* __restrict__ w, const float* __restrict__ dy, int n,
+                                              int S2, float inv_n, float* dq, bf16* vext4, float* loss, float* gb2) {
     const int i = blockIdx.x * 256 + threadIdx.x;
     float l = 0.f, d = 0.f;
     if (i < n) {
+        const int b = i / S2, p = i - b * S2;
         if (target) {
-            const float e = q[i] - target[i];
-            l = e * e * inv_n;
-            d = 2.f * e * inv_n;
+            const float e = q[i] - target[i], wb = w ? w[b] : 1.f;
+            l = wb * e * e * inv_n;
+            d = 2.f * wb * e * inv_n;
         } else {
             d = dy[i];
         }
         dq[i] = d;
-        const int b = i / S2, p = i - b * S2;
         vext4[((size_t)b * VC + 33) * S2 + p] = __float2bfloat16_rn(d);
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -704,11 +705,11 @@ int backward(fi_fno* h, int B) {
     return FI_OK;
 }
 
-int set_loss(fi_fno* h, int B, const float* target, const float* dy) {
+int set_loss(fi_fno* h, int B, const float* target, const float* w, const float* dy) {
     const int n = B * h->S2;
     FNO_CK(cudaMemsetAsync(h->grads, 0, sizeof(float) * h->o.total, h->st));
     FNO_CK(cudaMemsetAsync(h->scal, 0, sizeof(float) * 4, h->st));
-    k_loss<<<(n + 255) / 256, 256, 0, h->st>>>(h->q, target, dy, n, h->S2, 1.f / n, h->dq, h->vext[NLAYER],
+    k_loss<<<(n + 255) / 256, 256, 0, h->st>>>(h->q, target, w, dy, n, h->S2, 1.f / n, h->dq, h->vext[NLAYER],
                                                h->scal, h->grads + h->o.b2);
     FNO_CK(cudaGetLastError());
     return FI_OK;
@@ -864,18 +865,23 @@ int fi_fno_backward(fi_fno* h, int32_t B, const float* dy) {
     if (!h || !dy) return fail(h, FI_ERR_ARG, "null pointer");
     if (B != h->fwdB) return fail(h, FI_ERR_STATE, "backward needs a forward pass of the same batch");
     FNO_CK(cudaSetDevice(h->device));
-    int rc = set_loss(h, B, nullptr, dy);
+    int rc = set_loss(h, B, nullptr, nullptr, dy);
     if (!rc) rc = backward(h, B);
     return rc ? rc : finish(h);
 }
 
 int fi_fno_train_step(fi_fno* h, int32_t B, const float* x, const float* target, float lr, float* loss) {
+    return fi_fno_train_step_weighted(h, B, x, target, nullptr, lr, loss);
+}
+
+int fi_fno_train_step_weighted(fi_fno* h, int32_t B, const float* x, const float* target, const float* w, float lr,
+                               float* loss) {
     if (!h || !x || !target) return fail(h, FI_ERR_ARG, "null pointer");
     int rc = check_batch(h, B);
     if (rc) return rc;
     FNO_CK(cudaSetDevice(h->device));
     rc = forward(h, B, x, h->q);
-    if (!rc) rc = set_loss(h, B, target, nullptr);
+    if (!rc) rc = set_loss(h, B, target, w, nullptr);
     if (!rc) rc = backward(h, B);
     if (!rc) rc = adam(h, lr);
     if (!rc) rc = finish(h);

@@ -114,14 +114,16 @@ class FNO:
         self._sync_producer()
         self._check(self._lib.fi_fno_backward(self._h, B, dp), "fi_fno_backward")
 
-    def train_step(self, x, target, lr: float) -> float:
-        """Forward, mean-squared-error loss, backward and one Adam step; returns the loss."""
+    def train_step(self, x, target, lr: float, weights=None) -> float:
+        """Forward, mean-squared-error loss (per-sample weights [B] if given), backward and
+        one Adam step; returns the loss."""
         B = x.shape[0]
         xp = self._tensor(x, (B, N_IN, self.S, self.S), "x")
         tp = self._tensor(target, (B, self.S, self.S), "target")
+        wp = None if weights is None else self._tensor(weights, (B,), "weights")
         loss = C.c_float(0.0)
         self._sync_producer()
-        self._check(self._lib.fi_fno_train_step(self._h, B, xp, tp, C.c_float(lr), C.byref(loss)),
+        self._check(self._lib.fi_fno_train_step_weighted(self._h, B, xp, tp, wp, C.c_float(lr), C.byref(loss)),
                     "fi_fno_train_step")
         return float(loss.value)
 

@@ -297,6 +297,10 @@ int fi_fno_forward(fi_fno* h, int32_t B, const float* x, float* y);
 int fi_fno_backward(fi_fno* h, int32_t B, const float* dy);
 /* forward, mean-squared-error loss against target [B][S][S], backward, one Adam step */
 int fi_fno_train_step(fi_fno* h, int32_t B, const float* x, const float* target, float lr, float* loss);
+/* the same with per-sample loss weights w [B] (device): loss = mean over samples and
+ * cells of w_b (y - target)^2 */
+int fi_fno_train_step_weighted(fi_fno* h, int32_t B, const float* x, const float* target, const float* w,
+                               float lr, float* loss);
 int fi_fno_adam(fi_fno* h, float lr); /* one Adam step with the current gradients */
 int fi_fno_set_adam(fi_fno* h, float beta1, float beta2, float eps); /* default 0.9, 0.999, 1e-8 */
 const char* fi_fno_last_error(const fi_fno* h);

@@ -153,10 +153,12 @@ def backward(params, cache, dq):
     return g
 
 
-def mse(q, target):
-    """Mean-squared error and its gradient with respect to q."""
+def mse(q, target, w=None):
+    """Mean-squared error (per-sample weights w [B] if given) and its gradient w.r.t. q."""
     e = np.asarray(q, dtype=np.float64) - target
-    return float(np.mean(e * e)), 2.0 * e / e.size
+    wb = np.ones(e.shape[0]) if w is None else np.asarray(w, dtype=np.float64)
+    we = wb[:, None, None] * e
+    return float(np.mean(we * e)), 2.0 * we / e.size
 
 
 def init_params(seed=0, scale_spec=None):

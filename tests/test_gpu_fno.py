@@ -107,6 +107,26 @@ def test_train_step_loss_and_descent(torch):
     net.close()
 
 
+def test_weighted_loss_matches_oracle(torch):
+    S, B = 32, 4
+    net, p = _net(S, B, seed=21)
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal((B, 6, S, S)).astype(np.float32)
+    t = rng.standard_normal((B, S, S)).astype(np.float32)
+    w = np.array([0.5, 2.0, 1.0, 0.1], dtype=np.float32)
+    loss = net.train_step(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda(), 0.0,
+                          weights=torch.from_numpy(w).cuda())
+    q, cache = O.forward(p, x)
+    want, dq = O.mse(q, t, w)
+    assert abs(loss - want) / want < 2 * FWD_TOL
+    g = net.get_grads()   # gradients of this step (lr 0 leaves the parameters)
+    gref = O.backward(p, cache, dq)
+    for name in ("W0", "Wloc2", "Q1", "b2"):
+        a, b = _groups()[name]
+        assert _rel(g[a:b], gref[a:b]) < GRAD_TOL, name
+    net.close()
+
+
 def test_batch_limits(torch):
     from fastiso_b200 import abi
     from fastiso_b200.fno import FNO

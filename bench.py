@@ -9,7 +9,8 @@ inputs resident on the device (CUDA-event time on the library's stream); `e2e` i
 same metric through the public coupling API (init_integrator / step! with an
 externally supplied ice field copied from host memory every step and the displacement
 read back).  Also reported: the plain FP64 form (the comparison baseline), the
-dominant kernel against the HBM roofline, and the CPU oracle timed on the host cores.
+dominant kernel against the HBM roofline, the surrogate network's training and inference
+throughput, the N=1024 high-resolution case, and the CPU oracle timed on the host cores.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -241,6 +242,21 @@ def ensemble_bench(dev, rank=0, world=1):
         ps.close()
     v = ENS_MEMBERS * ENS_WINDOW_YR / 1e3 / (ms / 1e3)
     plain = tot_kyr / (tot_ms / 1e3)
+    # HBM roofline of k_ens: algorithmic bytes of every member's BS3 attempts in the window
+    # (3 right-hand sides each: rows_fwd + cols + rows_inv of its own N) over the window's
+    # device time (the slowest rank's)
+    byts = 0
+    for p in parts:
+        for i, att in zip(p["members"], p.get("attempts", [])):
+            N = members[i]["N"]
+            bpl = bytes_per_launch(N, N)
+            byts += 3 * att * (bpl["k_rows_fwd"] + bpl["k_cols"] + bpl["k_rows_inv"])
+    peak, kind = hbm_peak()
+    achieved = byts / (ms * 1e-3) / 1e9 if byts else None
+    roof = {"bound": "hbm", "kernel": "k_ens", "achieved": round(achieved, 1) if achieved else None,
+            "peak": peak, "peak_kind": kind, "unit": "GB/s",
+            "frac": round(achieved / peak, 4) if achieved else None, "bytes_per_window": byts,
+            "member_attempts": int(sum(sum(p.get("attempts", [])) for p in parts))}
     from fastiso_b200.autotune import tiles_for
 
     return {"value": v, "unit": "member-kyr/s", "members": ENS_MEMBERS, "ranks": world,
@@ -250,10 +266,10 @@ def ensemble_bench(dev, rank=0, world=1):
             "status_ok": ok, "ms": ms,
             "plain_fp64_loop": {"value": plain, "unit": "member-kyr/s",
                                 "sample": "4 members x 200 yr after 50 yr, one after another"},
-            "speedup_vs_plain_loop": v / plain}
+            "speedup_vs_plain_loop": v / plain, "roofline": roof}
 
 
-C5_WARM_YR, C5_TIMED_YR, C5_CMP_YR = 5.0, 20.0, 20.0
+C5_WARM_YR, C5_TIMED_YR, C5_CMP_YR = 5.0, 20.0, 500.0
 
 
 def config5_bench(dev):
@@ -307,6 +323,53 @@ def config5_bench(dev):
             "relL2_u_vs_fp64": float(np.linalg.norm(ua - ub) / max(np.linalg.norm(ub), 1e-300)),
             "u_finite": bool(np.isfinite(u32_end).all()),
             "clocks": clk.summary()}
+
+
+def fno_flops_per_sample(S=128, C=32, KX=16, KY=32, PW=128, nin=6, layers=4):
+    """Algorithmic FLOPs of one forward pass of the surrogate per sample (the GEMMs as
+    contracted, without padding): lift, per layer the DFT along x and y, the mode mixing,
+    the inverse along y and x and the pointwise path, the projection."""
+    S2 = S * S
+    layer = (2 * C * S * 2 * KX * S + 2 * KX * C * 2 * KY * 2 * S + 2 * KX * KY * 64 * 64
+             + 2 * C * KX * 2 * S * 2 * KY + 2 * S2 * C * C + 2 * C * S * S * 2 * KX)
+    return 2 * S2 * C * nin + layers * layer + 2 * S2 * PW * C + 2 * S2 * PW
+
+
+def fno_bench(dev, steps, warmup, S=128, B=32):
+    """The surrogate's own kernels: training steps (forward, loss, backward, Adam) and
+    forward passes on a synthetic batch of 32 samples of 6 x 128 x 128 (the config-4
+    shape), timed with CUDA events around the synchronous calls."""
+    import torch
+    from fastiso_b200.fno import FNO
+
+    g = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.randn(B, 6, S, S, generator=g).cuda(dev)
+    t = torch.randn(B, S, S, generator=g).cuda(dev)
+    net = FNO(S=S, max_batch=B, device=dev, seed=0)
+    for _ in range(warmup):
+        net.train_step(x, t, 1e-4)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize(dev)
+    ev[0].record()
+    for _ in range(steps):
+        net.train_step(x, t, 1e-4)
+    ev[1].record()
+    y = net.forward(x)
+    for _ in range(warmup):
+        net.forward(x, out=y)
+    ev[2].record()
+    for _ in range(steps):
+        net.forward(x, out=y)
+    ev[3].record()
+    torch.cuda.synchronize(dev)
+    net.close()
+    train_ms = ev[0].elapsed_time(ev[1]) / steps
+    fwd_ms = ev[2].elapsed_time(ev[3]) / steps
+    f = fno_flops_per_sample(S)
+    return {"train_samples_per_s": B / (train_ms / 1e3), "infer_samples_per_s": B / (fwd_ms / 1e3),
+            "train_ms_per_step": train_ms, "forward_ms_per_batch": fwd_ms, "batch": B, "S": S,
+            "forward_gflop_per_sample": f / 1e9,
+            "forward_tflops": f * B / (fwd_ms / 1e3) / 1e12}
 
 
 def cpu_oracle_sample(seconds_target=12.0, seg=5.0):
@@ -440,6 +503,9 @@ def run_gpu(args, rank, world, dev):
     # ---- roofline of the dominant kernel ----------------------------------------
     seg = max(1, c1["segments"] - c0["segments"])
     roof = roofline(dev, 1e3 * t_total / max(1, attempts), attempts / seg, c1["executor"], c1["grid"])
+    # ---- the surrogate network and the N = 1024 case (outside the timed region) ----
+    surrogate = fno_bench(dev, 20, max(3, args.warmup))
+    config5 = config5_bench(dev)
     # ---- CPU baseline (oracle) ---------------------------------------------------
     cpu_v, cores, yrs = cpu_oracle_sample()
     line = {
@@ -460,6 +526,8 @@ def run_gpu(args, rank, world, dev):
                        "sample": "20 yr after 20 yr warm-up"},
         "speedup_vs_plain_fp64": value / world / plain_kyr_s,
         "ensemble": ens,
+        "surrogate": surrogate,
+        "config5": config5,
         "e2e": {"value": e2e_val, "unit": "kyr/s", "h2d_bytes_per_step": 8 * N350 * N350,
                 "d2h_bytes_per_step": 8 * N350 * N350,
                 "path": "init_integrator + per step: set H_ice (host) -> step!(1 kyr) -> read u (host)"},
@@ -483,6 +551,10 @@ def main():
                     help="small config-3 ensemble (16 members, 20 yr) for an ncu capture of k_ens")
     ap.add_argument("--profile", action="store_true",
                     help="only a short fused N=350 segment (10 yr warm-up + 5 yr) for ncu captures")
+    ap.add_argument("--fno", action="store_true",
+                    help="only the surrogate network's training and inference throughput (128^2, batch 32)")
+    ap.add_argument("--profile-config5", action="store_true",
+                    help="N=1024: 5 yr warm-up launch, then one 0.2-yr launch of k_persist (ncu capture target)")
     ap.add_argument("--config5", action="store_true",
                     help="only the N=1024 high-resolution case (short window, roofline, rel-L2 vs FP64)")
     args = ap.parse_args()
@@ -510,8 +582,19 @@ def main():
                           "steps": [sm.stats()["naccept"] + sm.stats()["nreject"] for sm in sims]}))
         ens.close()
         return
+    if args.fno:
+        print(json.dumps({"fno": fno_bench(local, args.steps, args.warmup)}), flush=True)
+        return
     if args.config5:
         print(json.dumps({"config5": config5_bench(local)}), flush=True)
+        return
+    if args.profile_config5:
+        sim = W.config5(form="fp32")
+        sim.cfg.device = local
+        integ = F.init_integrator(sim)
+        F.step(integ, 5.0, True)
+        F.step(integ, 0.2, True)
+        print(json.dumps({"profile_case": "config5 N=1024 fp32, 5 yr + 0.2 yr", "stats": sim.stats()}))
         return
     if args.profile:
         sim = W.config2(form="fp32", N=N350)

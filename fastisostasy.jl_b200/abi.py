@@ -220,7 +220,7 @@ _SIGS = {
     "fi_ensemble_trace": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "fi_ensemble_destroy": (None, [C.c_void_p]),
     "fi_fno_gemm": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
-                             C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int64]),
+                             C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_int32]),
     "fi_fno_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]),
     "fi_fno_num_params": (C.c_int64, [C.c_void_p]),
     "fi_fno_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),

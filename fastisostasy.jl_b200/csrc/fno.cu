@@ -14,16 +14,17 @@
 //   DFT along x:   v[(b,c,y)][x]            x F1[(part,kx)][x]            -> T
 //   DFT along y:   T[(kx,b,c)][(part,y)]    x F2[(kyi,part')][(part,y)]   -> Z (per mode)
 //   channel mix:   Z[mode][b][(part,ci)]    x Wmat[mode][(part',co)][(part,ci)]  (512 batches)
-//   inverse y:     Y[(b,co,kx)][(kyi,part)] x G2[(part',y)][(kyi,part)]   -> G
-//   inverse x:     G[(b,co,y)][(kx,part)]   x G1[x][(kx,part)]            -> + local path, bias, GELU
+//   inverse y:     Y[(b,co,kx)][(kyi,part)] x G2[(part',y)][(kyi,part)]   -> G[(b,y)][co][(kx,part)]
+//   inverse x + pointwise path, one GEMM per row (b, y) of pixels x channels with K = 32 + 32:
+//                  [G1[x][(kx,part)] | v[b][ci][y][x]]  x  [G[(b,y)][co][(kx,part)] | Wloc[co][ci]]
+//                  (the activation v read in place from NCHW as an MN-major operand)
 // The backward pass runs the same GEMMs against the transposed matrices, and the weight
 // gradients of the pointwise layers are split-K GEMMs over pixels whose B operand carries a
 // row of ones (bias gradient) and, for the projection, the loss gradient (dQ2).
 //
-// Activations are kept twice, NCHW ([b][c][y*S+x], the DFT's operand) and NHWC
-// ([(b,p)][c], the pointwise layers' operand); the epilogue of the producing GEMM writes
-// both.  All parameters are FP32 masters (Adam), packed to BF16 operand copies after each
-// update.
+// Activations live in NCHW ([b][c][y*S+x]) only: the pointwise layers and the projection
+// read them as MN-major operands (pixels x channels).  All parameters are FP32 masters
+// (Adam), packed to BF16 operand copies after each update.
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -93,21 +94,15 @@ __device__ __forceinline__ void store16(bf16* dst, const float* v) {
 // GEMM epilogues (called per row and 16-column chunk; every N below is a multiple of 16)
 // ---------------------------------------------------------------------------
 
-// lift: row (b, p), col c -> v0 in NCHW and NHWC
+// lift: batch z = b, row p, col c -> v0 in NCHW
 struct EpiLift {
     bf16* vext;
-    bf16* vnhwc;
     const float* bias;
     int S2;
-    __device__ __forceinline__ void operator()(int, int row, int c0, const float* v, int) const {
-        float w[16];
+    __device__ __forceinline__ void operator()(int z, int p, int c0, const float* v, int) const {
+        bf16* o = vext + ((size_t)z * VC + c0) * S2 + p;
 #pragma unroll
-        for (int i = 0; i < 16; i++) w[i] = v[i] + bias[c0 + i];
-        const int b = row / S2, p = row - b * S2;
-        store16(vnhwc + (size_t)row * C + c0, w);
-        bf16* o = vext + ((size_t)b * VC + c0) * S2 + p;
-#pragma unroll
-        for (int i = 0; i < 16; i++) o[(size_t)i * S2] = __float2bfloat16_rn(w[i]);
+        for (int i = 0; i < 16; i++) o[(size_t)i * S2] = __float2bfloat16_rn(v[i] + bias[c0 + i]);
     }
     __device__ __forceinline__ void row_done(int, int) const {}
 };
@@ -169,16 +164,16 @@ struct EpiMix {
 };
 
 // inverse DFT along y (and the adjoint of the DFT along y): row (b, c, kx), col n = part*S + y,
-// out G[b][c][y][kx*2 + part]
+// out G[(b, y)][c][kx*2 + part]
 struct EpiIdftY {
     bf16* G;
     int S;
     __device__ __forceinline__ void operator()(int, int row, int n0, const float* v, int) const {
-        const int bc = row / KX, kx = row - bc * KX;
+        const int bc = row / KX, kx = row - bc * KX, b = bc / C, c = bc - b * C;
         const int part = n0 / S, y0 = n0 - part * S;
 #pragma unroll
         for (int i = 0; i < 16; i++)
-            G[((size_t)bc * S + y0 + i) * 32 + kx * 2 + part] = __float2bfloat16_rn(v[i]);
+            G[(((size_t)b * S + y0 + i) * C + c) * 32 + kx * 2 + part] = __float2bfloat16_rn(v[i]);
     }
     __device__ __forceinline__ void row_done(int, int) const {}
 };
@@ -201,60 +196,58 @@ struct EpiNchw {
     __device__ __forceinline__ void row_done(int, int) const {}
 };
 
-// inverse DFT along x + local path + bias: row (b, c, y), col x.  Saves z (FP32) and writes
-// the activation in NCHW and NHWC.
-struct EpiIdftX {
-    const float* L;
+// inverse DFT along x + pointwise path + bias: batch z = (b, y), row x, col c.  Saves z
+// (FP32) and writes the activation, both NCHW.
+struct EpiPixAct {
     const float* bias;
     float* zs;
     bf16* vext;
-    bf16* vnhwc;
     int S, S2, act;
-    __device__ __forceinline__ void operator()(int, int row, int x0, const float* v, int) const {
-        const int bc = row / S, y = row - bc * S, b = bc / C, c = bc - b * C;
-        const size_t base = (size_t)row * S + x0;  // = (b*C + c)*S2 + y*S + x0
-        const float bi = bias[c];
-        const float4* l4 = reinterpret_cast<const float4*>(L + base);
-        float4* z4 = reinterpret_cast<float4*>(zs + base);
-        float w[16];
+    __device__ __forceinline__ void operator()(int z, int x, int c0, const float* v, int) const {
+        const int b = z / S, y = z - b * S;
+        const size_t p = (size_t)y * S + x;
+        float* zo = zs + ((size_t)b * C + c0) * S2 + p;
+        bf16* vo = vext + ((size_t)b * VC + c0) * S2 + p;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const float4 l = l4[q];
-            float4 zz;
-            zz.x = v[4 * q] + l.x + bi;
-            zz.y = v[4 * q + 1] + l.y + bi;
-            zz.z = v[4 * q + 2] + l.z + bi;
-            zz.w = v[4 * q + 3] + l.w + bi;
-            z4[q] = zz;
-            w[4 * q] = act ? gelu(zz.x) : zz.x;
-            w[4 * q + 1] = act ? gelu(zz.y) : zz.y;
-            w[4 * q + 2] = act ? gelu(zz.z) : zz.z;
-            w[4 * q + 3] = act ? gelu(zz.w) : zz.w;
+        for (int i = 0; i < 16; i++) {
+            const float zz = v[i] + bias[c0 + i];
+            zo[(size_t)i * S2] = zz;
+            vo[(size_t)i * S2] = __float2bfloat16_rn(act ? gelu(zz) : zz);
         }
-        store16(vext + ((size_t)b * VC + c) * S2 + (size_t)y * S + x0, w);
-        bf16* h = vnhwc + ((size_t)b * S2 + (size_t)y * S + x0) * C + c;
-#pragma unroll
-        for (int i = 0; i < 16; i++) h[(size_t)i * C] = __float2bfloat16_rn(w[i]);
     }
     __device__ __forceinline__ void row_done(int, int) const {}
 };
 
-// projection: row (b, p), col j (all 128 in one tile): q = sum_j GELU(a_j + b1_j) Q2_j + b2
+// batch z = (b, y), row x, col c -> out[b][c][y*S + x] (FP32)
+struct EpiPixStore {
+    float* out;
+    int S, S2;
+    __device__ __forceinline__ void operator()(int z, int x, int c0, const float* v, int) const {
+        const int b = z / S, y = z - b * S;
+        float* o = out + ((size_t)b * C + c0) * S2 + (size_t)y * S + x;
+#pragma unroll
+        for (int i = 0; i < 16; i++) o[(size_t)i * S2] = v[i];
+    }
+    __device__ __forceinline__ void row_done(int, int) const {}
+};
+
+// projection: batch z = b, row p, col j (all 128 in one tile): q = sum_j GELU(a_j + b1_j) Q2_j + b2
 struct EpiProj {
     const float* b1;
     const float* Q2;
     const float* b2;
     float* q;
+    int S2;
     float acc;
     __device__ __forceinline__ void operator()(int, int, int j0, const float* v, int) {
 #pragma unroll
         for (int i = 0; i < 16; i++) acc += gelu(v[i] + b1[j0 + i]) * Q2[j0 + i];
     }
-    __device__ __forceinline__ void row_done(int, int row) { q[row] = acc + b2[0]; }
+    __device__ __forceinline__ void row_done(int z, int p) { q[(size_t)z * S2 + p] = acc + b2[0]; }
 };
 
-// projection adjoint (recomputes the hidden pre-activation a): da = dq Q2 GELU'(a) in
-// [(b,p)][j] and [b][j][p], the hidden GELU(a) in [b][128 + j][p]
+// projection adjoint (recomputes the hidden pre-activation a; batch z = b, row p):
+// da = dq Q2 GELU'(a) in [(b,p)][j] and [b][j][p], the hidden GELU(a) in [b][128 + j][p]
 struct EpiProjBwd {
     const float* b1;
     const float* Q2;
@@ -262,17 +255,19 @@ struct EpiProjBwd {
     bf16* da_rows;
     bf16* daT;
     int S2;
-    __device__ __forceinline__ void operator()(int, int row, int j0, const float* v, int) const {
-        const int b = row / S2, p = row - b * S2;
+    __device__ __forceinline__ void operator()(int b, int p, int j0, const float* v, int) const {
+        const size_t row = (size_t)b * S2 + p;
         const float g = dq[row];
         float d[16];
         bf16* t = daT + ((size_t)b * 2 * PW + j0) * S2 + p;
 #pragma unroll
         for (int i = 0; i < 16; i++) {
             const float a = v[i] + b1[j0 + i];
-            d[i] = g * Q2[j0 + i] * gelu_grad(a);
+            // Phi(a) once for GELU(a) = a Phi(a) and GELU'(a) = Phi(a) + a phi(a)
+            const float Phi = 0.5f * (1.f + erff(a * 0.70710678118654752f));
+            d[i] = g * Q2[j0 + i] * (Phi + a * 0.39894228040143268f * expf(-0.5f * a * a));
             t[(size_t)i * S2] = __float2bfloat16_rn(d[i]);
-            t[(size_t)(PW + i) * S2] = __float2bfloat16_rn(gelu(a));
+            t[(size_t)(PW + i) * S2] = __float2bfloat16_rn(a * Phi);
         }
         store16(da_rows + (size_t)row * PW + j0, d);
     }
@@ -283,17 +278,14 @@ struct EpiProjBwd {
 // element-wise and reduction kernels
 // ---------------------------------------------------------------------------
 
-// x [B][6][S2] FP32 -> NHWC [(b,p)][8] and NCHW [b][8][S2] BF16 (NCHW channel 6 = 1)
-__global__ void k_prep_input(const float* __restrict__ x, bf16* xn, bf16* xe, int B, int S2) {
+// x [B][6][S2] FP32 -> NCHW [b][8][S2] BF16 (channel 6 = 1 for the lift's bias gradient)
+__global__ void k_prep_input(const float* __restrict__ x, bf16* xe, int B, int S2) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)B * S2) return;
     const int b = (int)(i / S2), p = (int)(i - (size_t)b * S2);
-    float f[NIN];
 #pragma unroll
-    for (int c = 0; c < NIN; c++) f[c] = x[((size_t)b * NIN + c) * S2 + p];
-    reinterpret_cast<uint4*>(xn)[i] = make_uint4(pack2(f[0], f[1]), pack2(f[2], f[3]), pack2(f[4], f[5]), 0u);
-#pragma unroll
-    for (int c = 0; c < NIN; c++) xe[((size_t)b * XC + c) * S2 + p] = __float2bfloat16_rn(f[c]);
+    for (int c = 0; c < NIN; c++)
+        xe[((size_t)b * XC + c) * S2 + p] = __float2bfloat16_rn(x[((size_t)b * NIN + c) * S2 + p]);
     xe[((size_t)b * XC + 6) * S2 + p] = __float2bfloat16_rn(1.f);
     xe[((size_t)b * XC + 7) * S2 + p] = __float2bfloat16_rn(0.f);
 }
@@ -406,16 +398,19 @@ __global__ void __launch_bounds__(256) k_spec_wgrad(const bf16* __restrict__ Z, 
     }
 }
 
-// split-K partials [z][MN] summed over z into grad[base + map[i]] (map < 0: not a parameter)
+// split-K partials [z][MN] summed over z and added to grad[base + map[i]] (map < 0: not a
+// parameter; grad is zeroed before the backward pass).  Block (x, y) sums the z range y of
+// gridDim.y for 256 consecutive i.
 __global__ void k_reduce_map(const float* __restrict__ part, int nz, int MN, const int* __restrict__ map,
                              float* grad, long long base) {
     const int i = blockIdx.x * 256 + threadIdx.x;
     if (i >= MN) return;
     const int t = map[i];
     if (t < 0) return;
+    const int per = (nz + gridDim.y - 1) / gridDim.y, z0 = blockIdx.y * per, z1 = min(nz, z0 + per);
     float s = 0.f;
-    for (int z = 0; z < nz; z++) s += part[(size_t)z * MN + i];
-    grad[base + t] = s;
+    for (int z = z0; z < z1; z++) s += part[(size_t)z * MN + i];
+    if (z1 > z0) atomicAdd(&grad[base + t], s);
 }
 
 __global__ void k_adam(float* p, const float* __restrict__ g, float* m, float* v, long long n, float lr, float b1,
@@ -431,18 +426,25 @@ __global__ void k_adam(float* p, const float* __restrict__ g, float* m, float* v
 }
 
 // spectral weights -> real 64 x 64 block matrices [[Wr, -Wi], [Wi, Wr]] (rows part'*32 + co,
-// cols part*32 + ci) and their transposes; grid (mode, layer)
+// cols part*32 + ci) and their transposes; grid (mode, layer).  The weights are read and
+// both matrices written along their rows, through a shared-memory copy of the mode.
 __global__ void __launch_bounds__(256) k_pack_spec(const float* __restrict__ params, long long off0, bf16* Wm,
                                                    bf16* WmT) {
+    __shared__ float w[2][C][C + 1];  // [re, im][ci][co]
     const int mode = blockIdx.x, l = blockIdx.y;
     const float* W = params + off0 + (long long)l * LAYER + (size_t)mode * 2 * C * C;
+    for (int i = threadIdx.x; i < 2 * C * C; i += 256) w[i >> 10][(i >> 5) & 31][i & 31] = W[i];
+    __syncthreads();
     const size_t o = ((size_t)l * NM + mode) * 4096;
     for (int i = threadIdx.x; i < 4096; i += 256) {
+        // Wm row n = (pO, co), col k = (pI, ci)
         const int n = i >> 6, k = i & 63, pO = n >> 5, co = n & 31, pI = k >> 5, ci = k & 31;
-        const float wr = W[ci * C + co], wi = W[C * C + ci * C + co];
-        const float val = pO == pI ? wr : (pO == 0 ? -wi : wi);
-        Wm[o + i] = __float2bfloat16_rn(val);
-        WmT[o + (size_t)k * 64 + n] = __float2bfloat16_rn(val);
+        const float wr = w[0][ci][co], wi = w[1][ci][co];
+        Wm[o + i] = __float2bfloat16_rn(pO == pI ? wr : (pO == 0 ? -wi : wi));
+        // WmT row k' = (pI, ci), col n' = (pO, co): WmT[k'][n'] = Wm[n'][k']
+        const int kk = i >> 6, nn = i & 63, pI2 = kk >> 5, ci2 = kk & 31, pO2 = nn >> 5, co2 = nn & 31;
+        const float wr2 = w[0][ci2][co2], wi2 = w[1][ci2][co2];
+        WmT[o + i] = __float2bfloat16_rn(pO2 == pI2 ? wr2 : (pO2 == 0 ? -wi2 : wi2));
     }
 }
 
@@ -456,7 +458,7 @@ __global__ void k_pack_small(const float* __restrict__ params, Offsets o, bf16* 
     }
     if (i < NLAYER * C * C) {
         const int l = i / (C * C), r = i - l * C * C, co = r / C, ci = r - co * C;
-        const float w = params[o.layer[l] + SPEC + r];
+        const float w = params[o.layer[0] + (long long)l * LAYER + SPEC + r];
         Wl[i] = __float2bfloat16_rn(w);
         WlT[(size_t)l * C * C + ci * C + co] = __float2bfloat16_rn(w);
     }
@@ -487,11 +489,9 @@ struct fi_fno {
     bf16 *F1 = nullptr, *F2 = nullptr, *G2 = nullptr, *G1 = nullptr, *F1T = nullptr, *F2T = nullptr,
          *G2T = nullptr, *G1T = nullptr;
     // activations (saved for the backward pass) and scratch
-    bf16 *xn = nullptr, *xe = nullptr, *vext[NLAYER + 1] = {}, *vnhwc[NLAYER + 1] = {}, *Tb = nullptr,
-         *Zm[NLAYER] = {}, *Yb = nullptr, *Gt = nullptr, *dz = nullptr, *dzh = nullptr, *dYm = nullptr,
-         *da_rows = nullptr, *daT = nullptr;
-    float *zs[NLAYER] = {}, *L = nullptr, *q = nullptr, *dq = nullptr, *dvf = nullptr, *part = nullptr,
-          *scal = nullptr;
+    bf16 *xe = nullptr, *vext[NLAYER + 1] = {}, *Tb = nullptr, *Zm[NLAYER] = {}, *Yb = nullptr, *Gt = nullptr,
+         *dz = nullptr, *dYm = nullptr, *da_rows = nullptr, *daT = nullptr;
+    float *zs[NLAYER] = {}, *q = nullptr, *dq = nullptr, *dvf = nullptr, *part = nullptr, *scal = nullptr;
     int *map_loc = nullptr, *map_proj = nullptr, *map_lift = nullptr, *err = nullptr;
     int fwdB = 0;  // batch of the last forward pass (0: none)
     std::vector<void*> allocs;
@@ -522,10 +522,37 @@ cudaError_t dalloc(fi_fno* h, T** p, size_t count) {
     return cudaMemset(q, 0, count * sizeof(T) + 16);
 }
 
+// operands: K-major (rows K-contiguous) and MN-major (NCHW read as pixels x channels)
+TcOperand opK(const bf16* p, int ld, long long s = 0, long long s2 = 0) {
+    TcOperand o;
+    o.p = p;
+    o.ld = ld;
+    o.s = s;
+    o.s2 = s2;
+    o.mn = 0;
+    return o;
+}
+TcOperand opMN(const bf16* p, int ld, long long s = 0, long long s2 = 0) {
+    TcOperand o = opK(p, ld, s, s2);
+    o.mn = 1;
+    return o;
+}
+
+// C[z] = A[z] B[z]^T over K columns (columns [K1, K) from A2, B2 when K1 > 0)
 template <class Epi>
-cudaError_t gemm(fi_fno* h, int M, int N, int K, const bf16* A, int lda, long long sA, const bf16* B, int ldb,
-                 long long sB, int batch, const Epi& epi, int zdiv = 1, long long sA2 = 0, long long sB2 = 0) {
-    TcGemmArgs g{M, N, K, A, B, lda, ldb, sA, sB, h->err, zdiv, sA2, sB2};
+cudaError_t gemm(fi_fno* h, int M, int N, int K, TcOperand A, TcOperand B, int batch, const Epi& epi, int zdiv = 1,
+                 TcOperand A2 = TcOperand(), TcOperand B2 = TcOperand(), int K1 = 0) {
+    TcGemmArgs g;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.A = A;
+    g.B = B;
+    g.A2 = A2;
+    g.B2 = B2;
+    g.K1 = K1;
+    g.zdiv = zdiv;
+    g.err = h->err;
     if (N <= 32) return launch_gemm_tc<32>(g, batch, epi, h->st);
     if (N <= 64) return launch_gemm_tc<64>(g, batch, epi, h->st);
     return launch_gemm_tc<128>(g, batch, epi, h->st);
@@ -636,25 +663,30 @@ int finish(fi_fno* h) {
 int forward(fi_fno* h, int B, const float* x, float* y) {
     const int S = h->S, S2 = h->S2;
     const Offsets& o = h->o;
-    const long long nb = (long long)B * S2;
-    k_prep_input<<<(unsigned)((nb + 255) / 256), 256, 0, h->st>>>(x, h->xn, h->xe, B, S2);
+    const long long nb = (long long)B * S2, vs = (long long)VC * S2;
+    k_prep_input<<<(unsigned)((nb + 255) / 256), 256, 0, h->st>>>(x, h->xe, B, S2);
     FNO_CK(cudaGetLastError());
-    FNO_CK(gemm(h, B * S2, C, XC, h->xn, XC, 0, h->Pb, XC, 0, 1, EpiLift{h->vext[0], h->vnhwc[0], h->params + o.bP, S2}));
+    // lift: per sample, pixels x inputs (MN-major) times P
+    FNO_CK(gemm(h, S2, C, XC, opMN(h->xe, S2, (long long)XC * S2), opK(h->Pb, XC), B,
+                EpiLift{h->vext[0], h->params + o.bP, S2}));
     for (int l = 0; l < NLAYER; l++) {
         const float* lp = h->params + o.layer[l];
-        FNO_CK(gemm(h, C * S, 2 * KX, S, h->vext[l], S, (long long)VC * S2, h->F1, S, 0, B,
-                    EpiDftX{h->Tb, B, S, 1}));
-        FNO_CK(gemm(h, KX * B * C, 2 * KY, 2 * S, h->Tb, 2 * S, 0, h->F2, 2 * S, 0, 1, EpiModes{h->Zm[l], B}));
-        FNO_CK(gemm(h, B, 64, 64, h->Zm[l], 64, (long long)B * 64, h->Wm + (size_t)l * NM * 4096, 64, 4096, NM,
-                    EpiMix{h->Yb}));
-        FNO_CK(gemm(h, B * C * KX, 2 * S, 64, h->Yb, 64, 0, h->G2, 64, 0, 1, EpiIdftY{h->Gt, S}));
-        FNO_CK(gemm(h, B * S2, C, C, h->vnhwc[l], C, 0, h->Wl + (size_t)l * C * C, C, 0, 1, EpiNchw{h->L, S2, 0}));
-        FNO_CK(gemm(h, B * C * S, S, 2 * KX, h->Gt, 2 * KX, 0, h->G1, 2 * KX, 0, 1,
-                    EpiIdftX{h->L, lp + SPEC + C * C, h->zs[l], h->vext[l + 1], h->vnhwc[l + 1], S, S2,
-                             l < NLAYER - 1 ? 1 : 0}));
+        // DFT along x: per sample, rows (c, y)
+        FNO_CK(gemm(h, C * S, 2 * KX, S, opK(h->vext[l], S, vs), opK(h->F1, S), B, EpiDftX{h->Tb, B, S, 1}));
+        // DFT along y: rows (kx, b, c)
+        FNO_CK(gemm(h, KX * B * C, 2 * KY, 2 * S, opK(h->Tb, 2 * S), opK(h->F2, 2 * S), 1, EpiModes{h->Zm[l], B}));
+        // channel mixing, one batch per mode
+        FNO_CK(gemm(h, B, 64, 64, opK(h->Zm[l], 64, (long long)B * 64), opK(h->Wm + (size_t)l * NM * 4096, 64, 4096),
+                    NM, EpiMix{h->Yb}));
+        // inverse along y: rows (b, c, kx) -> G[(b, y)][c][(kx, part)]
+        FNO_CK(gemm(h, B * C * KX, 2 * S, 64, opK(h->Yb, 64), opK(h->G2, 64), 1, EpiIdftY{h->Gt, S}));
+        // inverse along x + pointwise path: batch (b, y), rows x, K = (kx, part) | ci
+        FNO_CK(gemm(h, S, C, 64, opK(h->G1, 2 * KX), opK(h->Gt, 2 * KX, (long long)S * C * 32, (long long)C * 32),
+                    B * S, EpiPixAct{lp + SPEC + C * C, h->zs[l], h->vext[l + 1], S, S2, l < NLAYER - 1 ? 1 : 0}, S,
+                    opMN(h->vext[l], S2, vs, S), opK(h->Wl + (size_t)l * C * C, C), 2 * KX));
     }
-    FNO_CK(gemm(h, B * S2, PW, C, h->vnhwc[NLAYER], C, 0, h->Q1b, C, 0, 1,
-                EpiProj{h->params + o.b1, h->params + o.Q2, h->params + o.b2, y, 0.f}));
+    FNO_CK(gemm(h, S2, PW, C, opMN(h->vext[NLAYER], S2, vs), opK(h->Q1b, C), B,
+                EpiProj{h->params + o.b1, h->params + o.Q2, h->params + o.b2, y, S2, 0.f}));
     h->fwdB = B;
     return FI_OK;
 }
@@ -663,44 +695,47 @@ int forward(fi_fno* h, int B, const float* x, float* y) {
 int backward(fi_fno* h, int B) {
     const int S = h->S, S2 = h->S2, SL = h->SL, ns = h->ns;
     const Offsets& o = h->o;
+    const long long vs = (long long)VC * S2, cs = (long long)C * S2;
     float* gr = h->grads;
     bf16* v4 = h->vext[NLAYER];
-    // projection
-    FNO_CK(gemm(h, B * S2, PW, C, h->vnhwc[NLAYER], C, 0, h->Q1b, C, 0, 1,
+    // projection: recompute the hidden layer, da and GELU(a); weights by split-K over pixels
+    FNO_CK(gemm(h, S2, PW, C, opMN(v4, S2, vs), opK(h->Q1b, C), B,
                 EpiProjBwd{h->params + o.b1, h->params + o.Q2, h->dq, h->da_rows, h->daT, S2}));
-    FNO_CK(gemm(h, 2 * PW, VC, SL, h->daT, S2, (long long)2 * PW * S2, v4, S2, (long long)VC * S2, B * ns,
-                EpiStoreF32{h->part, VC, (long long)2 * PW * VC}, ns, SL, SL));
-    k_reduce_map<<<(2 * PW * VC + 255) / 256, 256, 0, h->st>>>(h->part, B * ns, 2 * PW * VC, h->map_proj, gr, 0);
+    FNO_CK(gemm(h, 2 * PW, VC, SL, opK(h->daT, S2, (long long)2 * PW * S2, SL), opK(v4, S2, vs, SL), B * ns,
+                EpiStoreF32{h->part, VC, (long long)2 * PW * VC}, ns));
+    k_reduce_map<<<dim3((2 * PW * VC + 255) / 256, 16), 256, 0, h->st>>>(h->part, B * ns, 2 * PW * VC, h->map_proj,
+                                                                        gr, 0);
     FNO_CK(cudaGetLastError());
-    FNO_CK(gemm(h, B * S2, C, PW, h->da_rows, PW, 0, h->Q1Tb, PW, 0, 1, EpiNchw{h->dvf, S2, 0}));
+    FNO_CK(gemm(h, B * S2, C, PW, opK(h->da_rows, PW), opK(h->Q1Tb, PW), 1, EpiNchw{h->dvf, S2, 0}));
     for (int l = NLAYER - 1; l >= 0; l--) {
-        k_act_bwd<<<B * (S2 / 64), 256, 0, h->st>>>(h->dvf, l < NLAYER - 1 ? h->zs[l] : nullptr, h->dz, h->dzh, S2);
+        k_act_bwd<<<B * (S2 / 64), 256, 0, h->st>>>(h->dvf, l < NLAYER - 1 ? h->zs[l] : nullptr, h->dz, nullptr, S2);
         FNO_CK(cudaGetLastError());
         // pointwise path weights and bias: [co][ci | ones]
-        FNO_CK(gemm(h, C, C + 1, SL, h->dz, S2, (long long)C * S2, h->vext[l], S2, (long long)VC * S2, B * ns,
-                    EpiStoreF32{h->part, C + 1, (long long)C * (C + 1)}, ns, SL, SL));
-        k_reduce_map<<<(C * (C + 1) + 255) / 256, 256, 0, h->st>>>(h->part, B * ns, C * (C + 1), h->map_loc, gr,
-                                                                   o.layer[l]);
+        FNO_CK(gemm(h, C, C + 1, SL, opK(h->dz, S2, cs, SL), opK(h->vext[l], S2, vs, SL), B * ns,
+                    EpiStoreF32{h->part, C + 1, (long long)C * (C + 1)}, ns));
+        k_reduce_map<<<dim3((C * (C + 1) + 255) / 256, 32), 256, 0, h->st>>>(h->part, B * ns, C * (C + 1),
+                                                                             h->map_loc, gr, o.layer[l]);
         FNO_CK(cudaGetLastError());
         // spectral path: adjoint of the inverse DFT along x, then along y
-        FNO_CK(gemm(h, B * C * S, 2 * KX, S, h->dz, S, 0, h->G1T, S, 0, 1, EpiDftX{h->Tb, B, S, 0}));
-        FNO_CK(gemm(h, KX * B * C, 2 * KY, 2 * S, h->Tb, 2 * S, 0, h->G2T, 2 * S, 0, 1, EpiModes{h->dYm, B}));
+        FNO_CK(gemm(h, B * C * S, 2 * KX, S, opK(h->dz, S), opK(h->G1T, S), 1, EpiDftX{h->Tb, B, S, 0}));
+        FNO_CK(gemm(h, KX * B * C, 2 * KY, 2 * S, opK(h->Tb, 2 * S), opK(h->G2T, 2 * S), 1, EpiModes{h->dYm, B}));
         k_spec_wgrad<<<NM, 256, 0, h->st>>>(h->Zm[l], h->dYm, gr + o.layer[l], B);
         FNO_CK(cudaGetLastError());
-        // adjoint of the channel mixing, the DFT along y, the DFT along x
-        FNO_CK(gemm(h, B, 64, 64, h->dYm, 64, (long long)B * 64, h->WmT + (size_t)l * NM * 4096, 64, 4096, NM,
-                    EpiMix{h->Yb}));
-        FNO_CK(gemm(h, B * C * KX, 2 * S, 64, h->Yb, 64, 0, h->F2T, 64, 0, 1, EpiIdftY{h->Gt, S}));
-        FNO_CK(gemm(h, B * C * S, S, 2 * KX, h->Gt, 2 * KX, 0, h->F1T, 2 * KX, 0, 1, EpiStoreF32{h->dvf, S, 0}));
-        // + the pointwise path
-        FNO_CK(gemm(h, B * S2, C, C, h->dzh, C, 0, h->WlT + (size_t)l * C * C, C, 0, 1, EpiNchw{h->dvf, S2, 1}));
+        // adjoint of the channel mixing and of the DFT along y
+        FNO_CK(gemm(h, B, 64, 64, opK(h->dYm, 64, (long long)B * 64), opK(h->WmT + (size_t)l * NM * 4096, 64, 4096),
+                    NM, EpiMix{h->Yb}));
+        FNO_CK(gemm(h, B * C * KX, 2 * S, 64, opK(h->Yb, 64), opK(h->F2T, 64), 1, EpiIdftY{h->Gt, S}));
+        // adjoint of the DFT along x + the pointwise path: batch (b, y), rows x, K = (kx, part) | co
+        FNO_CK(gemm(h, S, C, 64, opK(h->F1T, 2 * KX), opK(h->Gt, 2 * KX, (long long)S * C * 32, (long long)C * 32),
+                    B * S, EpiPixStore{h->dvf, S, S2}, S, opMN(h->dz, S2, cs, S), opK(h->WlT + (size_t)l * C * C, C),
+                    2 * KX));
     }
     // lift weights and bias: [c][inputs | ones | zero]
     k_act_bwd<<<B * (S2 / 64), 256, 0, h->st>>>(h->dvf, nullptr, h->dz, nullptr, S2);
     FNO_CK(cudaGetLastError());
-    FNO_CK(gemm(h, C, XC, SL, h->dz, S2, (long long)C * S2, h->xe, S2, (long long)XC * S2, B * ns,
-                EpiStoreF32{h->part, XC, (long long)C * XC}, ns, SL, SL));
-    k_reduce_map<<<1, 256, 0, h->st>>>(h->part, B * ns, C * XC, h->map_lift, gr, 0);
+    FNO_CK(gemm(h, C, XC, SL, opK(h->dz, S2, cs, SL), opK(h->xe, S2, (long long)XC * S2, SL), B * ns,
+                EpiStoreF32{h->part, XC, (long long)C * XC}, ns));
+    k_reduce_map<<<dim3(1, 64), 256, 0, h->st>>>(h->part, B * ns, C * XC, h->map_lift, gr, 0);
     FNO_CK(cudaGetLastError());
     return FI_OK;
 }
@@ -744,8 +779,7 @@ int fi_fno_create(int32_t S, int32_t max_batch, int32_t device, uint64_t seed, f
     h->maxB = max_batch;
     h->device = device;
     h->o = offsets();
-    h->SL = 2048;
-    while (h->S2 % h->SL) h->SL /= 2;  // S2 is a multiple of 1024
+    h->SL = 512;  // pixels per split-K slice of the weight gradients (S2 is a multiple of 1024)
     h->ns = h->S2 / h->SL;
     auto bad = [&](int rc) {
         fi_fno_destroy(h);
@@ -764,23 +798,21 @@ int fi_fno_create(int32_t S, int32_t max_batch, int32_t device, uint64_t seed, f
               dalloc(h, &h->G2, 128 * S) == cudaSuccess && dalloc(h, &h->G1, 32 * S) == cudaSuccess &&
               dalloc(h, &h->F1T, 32 * S) == cudaSuccess && dalloc(h, &h->F2T, 128 * S) == cudaSuccess &&
               dalloc(h, &h->G2T, 128 * S) == cudaSuccess && dalloc(h, &h->G1T, 32 * S) == cudaSuccess &&
-              dalloc(h, &h->xn, B * S2 * XC) == cudaSuccess && dalloc(h, &h->xe, B * XC * S2) == cudaSuccess &&
+              dalloc(h, &h->xe, B * XC * S2) == cudaSuccess &&
               dalloc(h, &h->Tb, (size_t)KX * B * C * 2 * S) == cudaSuccess &&
               dalloc(h, &h->Yb, (size_t)B * C * KX * 64) == cudaSuccess &&
               dalloc(h, &h->Gt, (size_t)B * C * S * 32) == cudaSuccess &&
-              dalloc(h, &h->dz, (size_t)B * C * S2) == cudaSuccess && dalloc(h, &h->dzh, (size_t)B * S2 * C) == cudaSuccess &&
+              dalloc(h, &h->dz, (size_t)B * C * S2) == cudaSuccess &&
               dalloc(h, &h->dYm, (size_t)NM * B * 64) == cudaSuccess &&
               dalloc(h, &h->da_rows, (size_t)B * S2 * PW) == cudaSuccess &&
               dalloc(h, &h->daT, (size_t)B * 2 * PW * S2) == cudaSuccess &&
-              dalloc(h, &h->L, (size_t)B * C * S2) == cudaSuccess && dalloc(h, &h->q, (size_t)B * S2) == cudaSuccess &&
+              dalloc(h, &h->q, (size_t)B * S2) == cudaSuccess &&
               dalloc(h, &h->dq, (size_t)B * S2) == cudaSuccess && dalloc(h, &h->dvf, (size_t)B * C * S2) == cudaSuccess &&
               dalloc(h, &h->part, (size_t)B * h->ns * 2 * PW * VC) == cudaSuccess &&
               dalloc(h, &h->scal, 4) == cudaSuccess && dalloc(h, &h->map_loc, C * (C + 1)) == cudaSuccess &&
               dalloc(h, &h->map_proj, 2 * PW * VC) == cudaSuccess && dalloc(h, &h->map_lift, C * XC) == cudaSuccess &&
               dalloc(h, &h->err, 1) == cudaSuccess;
-    for (int l = 0; l <= NLAYER && ok; l++)
-        ok = dalloc(h, &h->vext[l], (size_t)B * VC * S2) == cudaSuccess &&
-             dalloc(h, &h->vnhwc[l], (size_t)B * S2 * C) == cudaSuccess;
+    for (int l = 0; l <= NLAYER && ok; l++) ok = dalloc(h, &h->vext[l], (size_t)B * VC * S2) == cudaSuccess;
     for (int l = 0; l < NLAYER && ok; l++)
         ok = dalloc(h, &h->zs[l], (size_t)B * C * S2) == cudaSuccess &&
              dalloc(h, &h->Zm[l], (size_t)NM * B * 64) == cudaSuccess;

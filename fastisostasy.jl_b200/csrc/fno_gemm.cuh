@@ -1,22 +1,27 @@
 // fno_gemm.cuh -- BF16 x BF16 -> FP32 GEMM on the 5th-generation tensor cores (tcgen05)
 // for the Fourier-neural-operator surrogate.
 //
-//   C[m][n] = sum_k A[m][k] * B[n][k]      (A: M x K, B: N x K, both K-contiguous rows)
+//   C[z][m][n] = sum_k A[z][m][k] * B[z][n][k]
 //
-// One block of 128 threads computes a 128 x BN tile.  Per K chunk of 64 the block copies
-// its A and B rows into shared memory in the K-major, no-swizzle canonical layout of the
-// UMMA operand descriptors (8-row x 16-byte core matrices; the core matrices of one
-// 8-row group follow each other along K at LBO bytes, the 8-row groups at SBO bytes),
+// Each 128-thread block computes 128 x BN output tiles (one per block as launched below).
+// Per K chunk of 64 the block copies its A and B rows into shared memory with cp.async
+// (16-byte copies, zero-filled outside the matrix) in the no-swizzle canonical layout of
+// the UMMA operand descriptors (8-row x 16-byte core matrices; the core matrices of one
+// 8-row group follow each other along K at LBO bytes, the 8-row groups at SBO bytes);
 // one elected thread issues four tcgen05.mma (K = 16 each, kind::f16, BF16 inputs, FP32
-// accumulation in tensor memory) and commits them to an mbarrier; the chunks are double
-// buffered so the copy of chunk i+1 overlaps the MMAs of chunk i.  The epilogue reads the
+// accumulation in tensor memory) and commits them to an mbarrier.  Two stage buffers:
+// the copy of the next chunk -- of this tile or of the block's next tile -- is in flight
+// while the tensor cores run the current one and while the epilogue reads the finished
 // accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31, i.e. tile rows) and
 // hands each row's BN values to an epilogue functor.  Every mbarrier wait is bounded: on
-// expiry the block raises an error word, frees its tensor memory and returns.
+// expiry the block raises an error word, waits for its copies, frees its tensor memory and
+// returns.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "../../include/fastiso_b200.h"
 
@@ -123,29 +128,73 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
 // ---------------------------------------------------------------------------
 // the GEMM
 // ---------------------------------------------------------------------------
-struct TcGemmArgs {
-    int M, N, K;
-    const __nv_bfloat16* A;  // M x K, row pitch lda (elements)
-    const __nv_bfloat16* B;  // N x K, row pitch ldb
-    int lda, ldb;
-    long long sA, sB;        // batch strides (elements)
-    int* err;                // set to FI_ERR_TIMEOUT when a wait gives up
-    // Two-level batch (split-K reductions): with zdiv > 1 batch z reads
-    // A + (z / zdiv) * sA + (z % zdiv) * sA2, and likewise for B.
-    int zdiv;
-    long long sA2, sB2;
+// One GEMM operand.  K-major (mn = 0): element (r, k) of batch (z1, z2) at
+// p[z1 * s + z2 * s2 + r * ld + k], rows K-contiguous.  MN-major (mn = 1): at
+// p[z1 * s + z2 * s2 + k * ld + r], each K column contiguous along the rows (an NCHW
+// activation read as pixels x channels).  The tensor cores take either form: the shared
+// memory image keeps the same core-matrix grid and only the inside of each 128-byte
+// core matrix is transposed, which bit 15 (A) / 16 (B) of the instruction descriptor
+// announces.
+struct TcOperand {
+    const __nv_bfloat16* p = nullptr;
+    int ld = 0;
+    long long s = 0, s2 = 0;
+    int mn = 0;
 };
 
-// rows x 64 chunk of a K-contiguous operand into the canonical layout (zero outside)
+struct TcGemmArgs {
+    int M = 0, N = 0, K = 0;
+    TcOperand A, B;    // product columns [0, K1)
+    TcOperand A2, B2;  // product columns [K1, K) read at column k - K1 (unused when K1 == K)
+    int K1 = 0;        // multiple of 16; 0 means K
+    int batch = 1;
+    // two-level batch: with zdiv > 1 batch z is (z / zdiv, z % zdiv), else (z, 0)
+    int zdiv = 1;
+    int* err = nullptr;  // set to FI_ERR_TIMEOUT when a wait gives up
+};
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// rows x 64 chunk (product columns k0 .. k0 + 63) of one side (A or B) of the product
+// into the canonical layout at shared address dst, zero outside [0, nrows) x [0, K).
+// Column groups of 8 below K1 come from o1, the rest from o2 at column k - K1.  `safe`
+// is any valid global address (the source operand of a zero-filled copy, never read).
 template <int ROWS>
-__device__ __forceinline__ void tc_stage(unsigned char* dst, const __nv_bfloat16* src, int ld, int row0, int nrows,
-                                         int k0, int K) {
+__device__ __forceinline__ void tc_stage(uint32_t dst, const TcOperand& o1, const TcOperand& o2, int z1, int z2,
+                                         int row0, int nrows, int k0, int K, int K1, const void* safe) {
+    // K-major groups: one 16-byte copy = 8 consecutive K elements of one row
     for (int v = threadIdx.x; v < ROWS * 8; v += TC_THREADS) {
         const int r = v >> 3, kv = v & 7;
-        const int gr = row0 + r, gk = k0 + kv * 8;
-        uint4 val = make_uint4(0u, 0u, 0u, 0u);
-        if (gr < nrows && gk < K) val = *reinterpret_cast<const uint4*>(src + (size_t)gr * ld + gk);
-        *reinterpret_cast<uint4*>(dst + tc_operand_offset(ROWS, r, kv * 8)) = val;
+        const int gk = k0 + kv * 8;
+        const bool second = gk >= K1;
+        const TcOperand& o = second ? o2 : o1;
+        if (o.mn) continue;
+        const int gr = row0 + r, ck = second ? gk - K1 : gk;
+        const bool ok = gr < nrows && gk < K;
+        const void* src = ok ? (const void*)(o.p + (size_t)z1 * o.s + (size_t)z2 * o.s2 + (size_t)gr * o.ld + ck) : safe;
+        cp_async16(dst + tc_operand_offset(ROWS, r, kv * 8), src, ok);
+    }
+    // MN-major groups: one 16-byte copy = 8 consecutive rows of one K column, stored as
+    // row (k % 8) of core matrix (k / 8, r / 8)
+    constexpr int RV = ROWS / 8;
+    for (int v = threadIdx.x; v < RV * 64; v += TC_THREADS) {
+        const int kc = v / RV, rv = v - kc * RV;
+        const int gk = k0 + kc;
+        const bool second = gk >= K1;
+        const TcOperand& o = second ? o2 : o1;
+        if (!o.mn) continue;
+        const int gr = row0 + rv * 8, ck = second ? gk - K1 : gk;
+        const bool ok = gr < nrows && gk < K;
+        const void* src = ok ? (const void*)(o.p + (size_t)z1 * o.s + (size_t)z2 * o.s2 + (size_t)ck * o.ld + gr) : safe;
+        cp_async16(dst + (kc >> 3) * (ROWS * 16) + rv * 128 + (kc & 7) * 16, src, ok);
     }
 }
 
@@ -157,11 +206,13 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(TcGemmArgs g, Epi epi) {
     __shared__ uint32_t tmem_base;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
-    const int z1 = g.zdiv > 1 ? (int)blockIdx.z / g.zdiv : (int)blockIdx.z;
-    const int z2 = g.zdiv > 1 ? (int)blockIdx.z % g.zdiv : 0;
-    const __nv_bfloat16* A = g.A + (size_t)z1 * g.sA + (size_t)z2 * g.sA2;
-    const __nv_bfloat16* B = g.B + (size_t)z1 * g.sB + (size_t)z2 * g.sB2;
+    const int mt = (g.M + TC_BM - 1) / TC_BM, nt = (g.N + BN - 1) / BN;
+    const int nch = (g.K + TC_BK - 1) / TC_BK;
+    const int K1 = g.K1 > 0 ? g.K1 : g.K;
+    const long long ntiles = (long long)mt * nt * g.batch;
+    const long long my_tiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const long long njobs = my_tiles * nch;  // (tile, chunk) pairs of this block, chunk fastest
+    const uint32_t sbase = tc_smem_u32(smem);
     if (warp == 0) {
         tc_alloc(&tmem_base, BN < 32 ? 32 : BN);
         tc_relinquish();
@@ -177,48 +228,75 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(TcGemmArgs g, Epi epi) {
     tc_fence_after();
     const uint32_t tmem = tmem_base;
     const uint32_t idesc = tc_instr_desc(TC_BM, BN);
-    const int nchunks = (g.K + TC_BK - 1) / TC_BK;
-    for (int c = 0; c < nchunks; c++) {
-        const int s = c & 1;
-        unsigned char* sa = smem + s * STAGE;
-        unsigned char* sb = sa + A_BYTES;
-        if (c >= 2 && tid == 0 && !mbar_wait(&bars[s], ((c - 2) >> 1) & 1)) s_fail = 1;
-        __syncthreads();
-        if (s_fail) break;
-        tc_stage<TC_BM>(sa, A, g.lda, m0, g.M, c * TC_BK, g.K);
-        tc_stage<BN>(sb, B, g.ldb, n0, g.N, c * TC_BK, g.K);
+    // output tile and chunk of job j
+    auto job = [&](long long j, int& m0, int& n0, int& z, int& c) {
+        const long long tile = blockIdx.x + (j / nch) * gridDim.x;
+        c = (int)(j % nch);
+        const long long mn = tile % ((long long)mt * nt);
+        z = (int)(tile / ((long long)mt * nt));
+        m0 = (int)(mn % mt) * TC_BM;
+        n0 = (int)(mn / mt) * BN;
+    };
+    auto stage = [&](long long j) {
+        int m0, n0, z, c;
+        job(j, m0, n0, z, c);
+        const int z1 = g.zdiv > 1 ? z / g.zdiv : z, z2 = g.zdiv > 1 ? z % g.zdiv : 0;
+        const uint32_t sa = sbase + (uint32_t)(j & 1) * STAGE;
+        tc_stage<TC_BM>(sa, g.A, g.A2, z1, z2, m0, g.M, c * TC_BK, g.K, K1, g.A.p);
+        tc_stage<BN>(sa + A_BYTES, g.B, g.B2, z1, z2, n0, g.N, c * TC_BK, g.K, K1, g.A.p);
+        cp_async_commit();
+    };
+    if (njobs > 0) stage(0);
+    for (long long j = 0; j < njobs; j++) {
+        const int s = (int)(j & 1);
+        if (j + 1 < njobs) {
+            // the other stage buffer was last read by the MMAs of job j - 1
+            if (j >= 1 && tid == 0 && !mbar_wait(&bars[(j - 1) & 1], (uint32_t)(((j - 1) >> 1) & 1))) s_fail = 1;
+            __syncthreads();
+            if (s_fail) break;
+            stage(j + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
         fence_async_smem();
         __syncthreads();
+        int m0, n0, z, c;
+        job(j, m0, n0, z, c);
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t a0 = tc_smem_u32(sa), b0 = tc_smem_u32(sb);
+            const uint32_t a0 = sbase + (uint32_t)s * STAGE, b0 = a0 + A_BYTES;
 #pragma unroll
             for (int ks = 0; ks < TC_BK / 16; ks++) {
                 // K step ks covers core-matrix columns 2ks and 2ks + 1
                 const uint64_t da = tc_smem_desc(a0 + 2 * ks * (TC_BM * 16), TC_BM * 16, 128);
                 const uint64_t db = tc_smem_desc(b0 + 2 * ks * (BN * 16), BN * 16, 128);
-                tc_mma(tmem, da, db, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+                const bool second = c * TC_BK + ks * 16 >= K1;
+                const uint32_t amn = second ? g.A2.mn : g.A.mn, bmn = second ? g.B2.mn : g.B.mn;
+                tc_mma(tmem, da, db, idesc | (amn << 15) | (bmn << 16), (c > 0 || ks > 0) ? 1u : 0u);
             }
             tc_commit(&bars[s]);
         }
-    }
-    if (tid == 0 && !s_fail && nchunks > 0 && !mbar_wait(&bars[(nchunks - 1) & 1], ((nchunks - 1) >> 1) & 1))
-        s_fail = 1;
-    __syncthreads();
-    tc_fence_after();
-    if (!s_fail) {
-        // the epilogue is copied so that it may carry per-row state across its column chunks
-        Epi e = epi;
-        const int row = m0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            float v[16];
-            tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (row < g.M && n0 + c0 < g.N) e(blockIdx.z, row, n0 + c0, v, g.N - (n0 + c0));
+        if (c == nch - 1) {
+            // tile complete: wait for its MMAs, read the accumulator, hand rows to the epilogue
+            if (tid == 0 && !mbar_wait(&bars[s], (uint32_t)((j >> 1) & 1))) s_fail = 1;
+            __syncthreads();
+            if (s_fail) break;
+            tc_fence_after();
+            Epi e = epi;  // per tile: the epilogue may carry per-row state across its column chunks
+            const int row = m0 + warp * 32 + lane;
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                float v[16];
+                tc_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+                if (row < g.M && n0 + c0 < g.N) e(z, row, n0 + c0, v, g.N - (n0 + c0));
+            }
+            if (row < g.M) e.row_done(z, row);
+            tc_fence_before();
+            __syncthreads();  // the next tile's MMAs overwrite the accumulator
         }
-        if (row < g.M) e.row_done(blockIdx.z, row);
-    } else if (tid == 0 && g.err) {
-        atomicExch(g.err, FI_ERR_TIMEOUT);
     }
+    cp_async_wait<0>();
+    if (s_fail && tid == 0 && g.err) atomicExch(g.err, FI_ERR_TIMEOUT);
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tc_dealloc(tmem, BN < 32 ? 32 : BN);
@@ -231,12 +309,22 @@ struct EpiStoreF32 {
     long long sC;
     __device__ __forceinline__ void operator()(int z, int row, int col0, const float* v, int nvalid) const {
         float* c = C + (size_t)z * sC + (size_t)row * ldc + col0;
-        const int n = nvalid < 16 ? nvalid : 16;
-        for (int i = 0; i < n; i++) c[i] = v[i];
+        if (nvalid >= 16 && ((uintptr_t)c & 15) == 0) {
+            float4* c4 = reinterpret_cast<float4*>(c);
+#pragma unroll
+            for (int q = 0; q < 4; q++) c4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            return;
+        }
+#pragma unroll
+        for (int i = 0; i < 16; i++)
+            if (i < nvalid) c[i] = v[i];
     }
     __device__ __forceinline__ void row_done(int, int) const {}
 };
 
+// One block per output tile (the kernel also walks several tiles per block when the grid
+// is smaller; measured slower here, where most products have a single K chunk: separate
+// blocks overlap one tile's epilogue with another's MMAs through their own tensor memory).
 template <int BN, class Epi>
 inline cudaError_t launch_gemm_tc(const TcGemmArgs& g, int batch, const Epi& epi, cudaStream_t st) {
     constexpr int STAGE = (TC_BM + BN) * TC_BK * 2;
@@ -244,13 +332,19 @@ inline cudaError_t launch_gemm_tc(const TcGemmArgs& g, int batch, const Epi& epi
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev >= 32 || !(attr_set & (1u << dev))) {
+    if (dev >= 32) return cudaErrorInvalidDevice;
+    if (!(attr_set & (1u << dev))) {
         e = cudaFuncSetAttribute(k_gemm_tc<BN, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * STAGE);
         if (e != cudaSuccess) return e;
-        if (dev < 32) attr_set |= 1u << dev;
+        attr_set |= 1u << dev;
     }
-    dim3 grid((g.M + TC_BM - 1) / TC_BM, (g.N + BN - 1) / BN, batch);
-    k_gemm_tc<BN, Epi><<<grid, TC_THREADS, 2 * STAGE, st>>>(g, epi);
+    TcGemmArgs a = g;
+    a.batch = batch;
+    const long long ntiles =
+        (long long)((g.M + TC_BM - 1) / TC_BM) * ((g.N + BN - 1) / BN) * (long long)batch;
+    if (ntiles <= 0) return cudaSuccess;
+    if (ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k_gemm_tc<BN, Epi><<<(unsigned)ntiles, TC_THREADS, 2 * STAGE, st>>>(a, epi);
     return cudaGetLastError();
 }
 

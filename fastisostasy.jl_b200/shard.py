@@ -49,7 +49,7 @@ def run_shard(members, t_ice, mod, years, rank, world, device=0, warm=50.0):
     from . import workloads as W
 
     mine = shard_members([m["N"] for m in members], world)[rank]
-    res = {"rank": rank, "members": mine, "status": [], "ms": 0.0}
+    res = {"rank": rank, "members": mine, "status": [], "ms": 0.0, "attempts": []}
     if mine:
         sims = [W.config3_simulation(members[i], t_ice, mod, form="fp32") for i in mine]
         for s in sims:
@@ -57,8 +57,12 @@ def run_shard(members, t_ice, mod, years, rank, world, device=0, warm=50.0):
             s.cfg.max_steps = 50_000_000
         ens = M.Ensemble(sims)
         ens.step(warm)
+        a0 = [s.stats() for s in sims]
         res["status"] = ens.step(years)
         res["ms"] = ens.last_gpu_ms
+        a1 = [s.stats() for s in sims]
+        # step attempts of each member in the timed window
+        res["attempts"] = [(b["naccept"] + b["nreject"]) - (a["naccept"] + a["nreject"]) for a, b in zip(a0, a1)]
         ens.close()
         for s in sims:
             s.close()

@@ -273,10 +273,12 @@ void fi_ensemble_destroy(fi_ensemble* e);
  * (tcgen05, BF16 inputs, FP32 accumulation in tensor memory), the channel-mixing and
  * truncated-DFT kernel of the surrogate, exposed for testing.  Device pointers; A is
  * M x K and B is N x K with K-contiguous rows (pitches lda, ldb, elements), C is M x N
- * FP32 (pitch ldc); sA, sB, sC are batch strides in elements.  K, lda, ldb, sA, sB must
- * be multiples of 8 and A, B 16-byte aligned (FI_ERR_ARG otherwise). */
+ * FP32 (pitch ldc); sA, sB, sC are batch strides in elements.  flags bit 0: A is
+ * MN-major (element (m, k) at A[k*lda + m]), bit 1: B is MN-major (element (n, k) at
+ * B[k*ldb + n]).  K, lda, ldb, sA, sB and an MN-major operand's M (N) must be multiples
+ * of 8 and A, B 16-byte aligned (FI_ERR_ARG otherwise). */
 int fi_fno_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32_t lda, const void* B, int32_t ldb,
-                float* C, int32_t ldc, int32_t batch, int64_t sA, int64_t sB, int64_t sC);
+                float* C, int32_t ldc, int32_t batch, int64_t sA, int64_t sB, int64_t sC, int32_t flags);
 
 /* The surrogate network: input x [B][6][S][S] FP32 (x fastest; the caller's normalised
  * fields), output y [B][S][S] FP32.  Lift 6 -> 32, four Fourier layers of width 32

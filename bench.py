@@ -548,7 +548,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fused", choices=["fused", "reference"])
     ap.add_argument("--profile-ensemble", action="store_true",
-                    help="small config-3 ensemble (16 members, 20 yr) for an ncu capture of k_ens")
+                    help="config-3 ensemble (--members, default 16; --years, default 20) for an ncu capture of k_ens")
+    ap.add_argument("--members", type=int, default=16)
+    ap.add_argument("--years", type=float, default=20.0)
     ap.add_argument("--profile", action="store_true",
                     help="only a short fused N=350 segment (10 yr warm-up + 5 yr) for ncu captures")
     ap.add_argument("--fno", action="store_true",
@@ -572,13 +574,14 @@ def main():
 
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.profile_ensemble:
-        members, t_ice, mod = W.config3_members(n_members=16)
+        members, t_ice, mod = W.config3_members(n_members=ENS_MEMBERS)
+        members = members[:args.members]
         sims = [W.config3_simulation(m, t_ice, mod, form="fp32") for m in members]
         for sm in sims:
             sm.cfg.device = local
         ens = F.Ensemble(sims)
-        ens.step(20.0)
-        print(json.dumps({"profile_case": "config3 16 members, 20 yr", "ms": ens.last_gpu_ms,
+        ens.step(args.years)
+        print(json.dumps({"profile_case": f"config3 {len(sims)} members, {args.years:g} yr", "ms": ens.last_gpu_ms,
                           "steps": [sm.stats()["naccept"] + sm.stats()["nreject"] for sm in sims]}))
         ens.close()
         return

@@ -200,6 +200,8 @@ _SIGS = {
     "fi_set_elastic_table": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fi_set_channel_scaling": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fi_set_tiles": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "fi_set_fft_schedule": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "fi_get_fft_schedule": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "fi_init": (C.c_int, [C.c_void_p]),
     "fi_rhs": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fi_rhs_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),

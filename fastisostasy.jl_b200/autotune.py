@@ -1,4 +1,4 @@
-"""Tile autotuner of the FP32 kernels (no counterpart in the reference).
+"""Tile and FFT-schedule autotuner of the FP32 kernels (no counterpart in the reference).
 
 The FP32 form's row phases work on tiles of ``h`` rows (row FFTs, stencils with a
 two-row halo) and its column phase on blocks of ``B`` spectral columns.  Small tiles
@@ -8,8 +8,15 @@ candidate (h, B) pairs on the actual workload with the library's own device time
 records the fastest per workload key in a JSON table shipped with the package
 (``tuning/b200.json``); ``tiles_for`` reads it back.
 
+The transforms (row and column FFTs of length N, padded convolutions of length M) run
+Stockham passes in a radix order; ``fft`` measures candidate orders of each length's
+factors (radices 2, 3, 4, 5, 7, 8, 16) per BS3 step of the single-simulation workload
+at that N and records the fastest as "fft:<L>"; ``fft_schedule_for`` reads it back and
+``Simulation`` applies it through fi_set_fft_schedule.
+
     python fastisostasy.jl_b200/autotune.py single 350     # config-2 grid (persistent executor)
     python fastisostasy.jl_b200/autotune.py ensemble 128   # config-3 ensemble
+    python fastisostasy.jl_b200/autotune.py fft 350        # radix order of the length-350 transforms
 """
 from __future__ import annotations
 
@@ -49,6 +56,97 @@ def tiles_for(key):
         return None
     v = _load().get(key)
     return tuple(v["tiles"]) if v else None
+
+
+def fft_schedule_for(L):
+    """The tuned radix order for transforms of length L, or None."""
+    if os.environ.get("FI_NO_TUNING") == "1":
+        return None
+    v = _load().get(f"fft:{L}")
+    return list(v["schedule"]) if v else None
+
+
+REG_RADICES = (16, 8, 7, 5, 4, 3, 2)
+
+
+def default_schedule(L):
+    """The library's default order (fi_api.cu: radix 8 while possible, then 4, 2, 7, 5,
+    3, larger odd factors)."""
+    m, out = L, []
+    for r in (8, 4, 2, 7, 5, 3):
+        while m % r == 0:
+            out.append(r)
+            m //= r
+    f = 11
+    while f * f <= m:
+        while m % f == 0:
+            out.append(f)
+            m //= f
+        f += 2
+    if m > 1:
+        out.append(m)
+    return out
+
+
+def schedule_candidates(L, limit=12, max_passes=6):
+    """Radix orders for length L: the library default, then the orderings of the
+    factorisations of L into register radices with the fewest passes first (at most
+    `limit` in all)."""
+    out = set()
+
+    def grow(m, acc):
+        if len(acc) > max_passes:
+            return
+        if m == 1:
+            out.add(tuple(acc))
+            return
+        for r in REG_RADICES:
+            if m % r == 0:
+                grow(m // r, acc + [r])
+
+    grow(L, [])
+    dflt = default_schedule(L)
+    cands = [c for c in sorted(out, key=lambda t: (len(t), t)) if list(c) != dflt]
+    return [dflt] + [list(c) for c in cands[:limit - 1]]
+
+
+def time_single_per_step(N, tiles=None, schedules=None, years=5.0, warm=5.0):
+    """Device ms per BS3 attempt of the config-2 workload at grid N (independent of the
+    step count, which the rounding of different schedules may change by a few steps)."""
+    sim = W.config2(form="fp32", N=N)
+    sim.tiles = tiles
+    sim.fft_schedules = dict(schedules or {})
+    sim.cfg.max_steps = 50_000_000
+    integ = M.init_integrator(sim)
+    M.step(integ, warm, True)
+    a0 = sim.stats()
+    M.step(integ, years, True)
+    a1 = sim.stats()
+    att = (a1["naccept"] + a1["nreject"]) - (a0["naccept"] + a0["nreject"])
+    sim.close()
+    return a1["last_gpu_ms"] / max(1, att)
+
+
+def tune_fft(N, write=True, limit=12):
+    """Radix orders of the length-N transforms (rows and columns of an N x N grid)."""
+    results = {}
+    for c in schedule_candidates(N, limit=limit):
+        try:
+            results[tuple(c)] = time_single_per_step(N, schedules={N: c})
+        except Exception as ex:
+            results[tuple(c)] = float("inf")
+            print(f"schedule {c}: {ex}", file=sys.stderr)
+        print(json.dumps({"kind": "fft", "L": N, "schedule": c, "ms_per_bs3_step": results[tuple(c)]}), flush=True)
+    best = min(results, key=results.get)
+    key = f"fft:{N}"
+    entry = {"schedule": list(best), "ms_per_unit": results[best], "unit": "ms per BS3 step (config-2 workload)",
+             "candidates": {"x".join(map(str, k)): v for k, v in results.items()}}
+    if write:
+        table = _load()
+        table[key] = entry
+        TABLE_DIR.mkdir(exist_ok=True)
+        TABLE.write_text(json.dumps(table, indent=1, sort_keys=True) + "\n")
+    return key, entry
 
 
 def time_single(N, tiles, years=20.0, warm=10.0):
@@ -105,5 +203,6 @@ def tune(kind, size, candidates=None, write=True):
 
 if __name__ == "__main__":
     kind = sys.argv[1] if len(sys.argv) > 1 else "single"
-    size = int(sys.argv[2]) if len(sys.argv) > 2 else (350 if kind == "single" else 128)
-    print(json.dumps(dict(zip(("key", "entry"), tune(kind, size)))))
+    size = int(sys.argv[2]) if len(sys.argv) > 2 else (128 if kind == "ensemble" else 350)
+    res = tune_fft(size) if kind == "fft" else tune(kind, size)
+    print(json.dumps(dict(zip(("key", "entry"), res))))

@@ -60,6 +60,7 @@ struct fi_handle {
     std::vector<void*> allocs;
     // FFT plans
     std::map<int, int> plan_of_len;
+    size_t n_plans_dev = 0;
     std::vector<Plan> plans;
     FftPlan* d_plans = nullptr;
     int plan_x, plan_y, plan_Mx, plan_My;
@@ -154,26 +155,38 @@ static int dalloc(fi_handle* h, T** p, size_t n) {
     return FI_OK;
 }
 
+// radix schedule of a plan (passes in order) and the fast-division constants of each pass
+static void plan_schedule(Plan& p, const int* radix, int np) {
+    p.npass = np;
+    for (int i = 0, Ns = 1; i < np; i++) {
+        p.radix[i] = radix[i];
+        p.mag_nb[i] = fastdiv_magic((unsigned)(p.L / radix[i]));
+        p.mag_ns[i] = fastdiv_magic((unsigned)Ns);
+        Ns *= radix[i];
+    }
+}
+
+// default schedule: radix 8 while possible, then 4, 2, 7, 5, 3, larger odd factors
+static int default_schedule(int L, int* radix) {
+    int m = L, np = 0;
+    while (m % 8 == 0) { radix[np++] = 8; m /= 8; }
+    while (m % 4 == 0) { radix[np++] = 4; m /= 4; }
+    while (m % 2 == 0) { radix[np++] = 2; m /= 2; }
+    const int small[3] = {7, 5, 3};
+    for (int q : small) while (m % q == 0) { radix[np++] = q; m /= q; }
+    for (int f = 11; f * f <= m; f += 2) while (m % f == 0) { radix[np++] = f; m /= f; }
+    if (m > 1) radix[np++] = m;
+    return np;
+}
+
 static int get_plan(fi_handle* h, int L, int* out) {
     auto it = h->plan_of_len.find(L);
     if (it != h->plan_of_len.end()) { *out = it->second; return FI_OK; }
     if (L < 1 || L > FFT_MAX_LEN) return set_err(h, FI_ERR_ARG, "transform length %d outside [1, %d]", L, FFT_MAX_LEN);
     Plan p{};
     p.L = L;
-    int m = L, np = 0;
-    while (m % 8 == 0) { p.radix[np++] = 8; m /= 8; }
-    while (m % 4 == 0) { p.radix[np++] = 4; m /= 4; }
-    while (m % 2 == 0) { p.radix[np++] = 2; m /= 2; }
-    const int small[3] = {7, 5, 3};
-    for (int q : small) while (m % q == 0) { p.radix[np++] = q; m /= q; }
-    for (int f = 11; f * f <= m; f += 2) while (m % f == 0) { p.radix[np++] = f; m /= f; }
-    if (m > 1) p.radix[np++] = m;
-    p.npass = np;
-    for (int i = 0, Ns = 1; i < np; i++) {
-        p.mag_nb[i] = fastdiv_magic((unsigned)(L / p.radix[i]));
-        p.mag_ns[i] = fastdiv_magic((unsigned)Ns);
-        Ns *= p.radix[i];
-    }
+    int radix[FFT_MAX_PASSES];
+    plan_schedule(p, radix, default_schedule(L, radix));
     std::vector<double2> t64(L);
     std::vector<float2> t32(L);
     for (int k = 0; k < L; k++) {
@@ -203,7 +216,10 @@ static int upload_plans(fi_handle* h) {
         v[i].tw32 = h->plans[i].tw32;
         v[i].tw64 = h->plans[i].tw64;
     }
-    RET(dalloc(h, &h->d_plans, v.size()));
+    if (!h->d_plans || h->n_plans_dev != v.size()) {
+        RET(dalloc(h, &h->d_plans, v.size()));
+        h->n_plans_dev = v.size();
+    }
     CK(cudaMemcpyAsync(h->d_plans, v.data(), v.size() * sizeof(FftPlan), cudaMemcpyHostToDevice, h->stream));
     return FI_OK;
 }
@@ -639,6 +655,38 @@ extern "C" int fi_set_tiles(fi_handle* h, int32_t h_rows, int32_t B_cols) {
     h->h_rows = h_rows;
     h->B_cols = B_cols;
     set_task_counts(h);
+    return FI_OK;
+}
+
+extern "C" int fi_set_fft_schedule(fi_handle* h, int32_t L, int32_t n, const int32_t* radices) {
+    if (!h) return FI_ERR_ARG;
+    cudaSetDevice(h->cfg.device);
+    if (h->initialized) return set_err(h, FI_ERR_STATE, "fi_set_fft_schedule must precede fi_init");
+    auto it = h->plan_of_len.find(L);
+    if (it == h->plan_of_len.end()) return set_err(h, FI_ERR_ARG, "%d is not a transform length of this grid", L);
+    if (n < 1 || n > FFT_MAX_PASSES || !radices) return set_err(h, FI_ERR_ARG, "schedule of %d passes", n);
+    long long prod = 1;
+    int radix[FFT_MAX_PASSES];
+    for (int i = 0; i < n; i++) {
+        if (radices[i] < 2) return set_err(h, FI_ERR_ARG, "radix %d < 2", radices[i]);
+        radix[i] = radices[i];
+        prod *= radices[i];
+        if (prod > L) break;
+    }
+    if (prod != L) return set_err(h, FI_ERR_ARG, "radices do not multiply to %d", L);
+    plan_schedule(h->plans[it->second], radix, n);
+    RET(upload_plans(h));
+    CK(cudaStreamSynchronize(h->stream));
+    return FI_OK;
+}
+
+extern "C" int fi_get_fft_schedule(fi_handle* h, int32_t L, int32_t* n, int32_t* radices) {
+    if (!h || !n || !radices) return FI_ERR_ARG;
+    auto it = h->plan_of_len.find(L);
+    if (it == h->plan_of_len.end()) return set_err(h, FI_ERR_ARG, "%d is not a transform length of this grid", L);
+    const Plan& p = h->plans[it->second];
+    *n = p.npass;
+    for (int i = 0; i < p.npass; i++) radices[i] = p.radix[i];
     return FI_OK;
 }
 

@@ -432,6 +432,9 @@ class Simulation:
         self.form = form
         self.cfg = cfg
         self.tiles = tiles
+        #: {transform length: [radix, ...]} applied at handle creation (FP32 and FP64
+        #: forms); lengths without an entry take the tuned table's schedule, if any
+        self.fft_schedules = {}
         self.elastic_table = get_greenintegrand_coeffs()
         self._handle = None
         self._initialized = False
@@ -483,6 +486,16 @@ class Simulation:
             self.tiles = tiles_for(f"single:{self.domain.nx}")
         if self.tiles is not None and self.cfg.form == abi.FI_FORM_FP32:
             self._check(lib.fi_set_tiles(h, int(self.tiles[0]), int(self.tiles[1])), "fi_set_tiles")
+        from .autotune import fft_schedule_for  # noqa: WPS433
+
+        lengths = {self.domain.nx, self.domain.ny, nextfastfft(2 * self.domain.nx - 1),
+                   nextfastfft(2 * self.domain.ny - 1)}
+        for L in sorted(lengths):
+            sched = self.fft_schedules.get(L)
+            if sched is None and self.cfg.form == abi.FI_FORM_FP32:
+                sched = fft_schedule_for(L)
+            if sched:
+                self.set_fft_schedule(L, sched)
         inp = self.prepared_inputs()
         for name, arr in inp["fields"].items():
             self.set_field(name, arr)
@@ -496,6 +509,18 @@ class Simulation:
         if ratio.size:
             self._check(lib.fi_set_channel_scaling(h, ratio.size, abi.dptr(ratio), abi.dptr(thick)),
                         "fi_set_channel_scaling")
+
+    def set_fft_schedule(self, L, radices):
+        """Radix order of the length-L transforms (before init_problem)."""
+        r = (C.c_int32 * len(radices))(*[int(x) for x in radices])
+        self._check(self.lib.fi_set_fft_schedule(self._handle, int(L), len(radices), r), "fi_set_fft_schedule")
+
+    def get_fft_schedule(self, L):
+        self._ensure_handle()
+        n = C.c_int32(0)
+        r = (C.c_int32 * 20)()
+        self._check(self.lib.fi_get_fft_schedule(self._handle, int(L), C.byref(n), r), "fi_get_fft_schedule")
+        return list(r[:n.value])
 
     def set_field(self, name, arr):
         self._ensure_handle()

@@ -181,6 +181,16 @@ int fi_set_channel_scaling(fi_handle* h, int32_t n, const double* visc_ratio_mea
  * differently). */
 int fi_set_tiles(fi_handle* h, int32_t h_rows, int32_t B_cols);
 
+/* No counterpart in the reference (which calls FFTW/CUFFT plans): the radix schedule of
+ * the library's transforms of length L (nx, ny or the padded convolution lengths Mx,
+ * My), between fi_create and fi_init.  radices[0..n) are the Stockham passes in order;
+ * they must multiply to L.  Radices 2, 3, 4, 5, 7, 8 and 16 run register butterflies,
+ * any other factor a generic O(R^2) pass.  The default is radix 8 while possible, then
+ * 4, 2, 7, 5, 3.  fastiso_b200.autotune measures schedules.  Results agree to rounding
+ * across schedules.  fi_get_fft_schedule writes the current one (at most 20 passes). */
+int fi_set_fft_schedule(fi_handle* h, int32_t L, int32_t n, const int32_t* radices);
+int fi_get_fft_schedule(fi_handle* h, int32_t L, int32_t* n, int32_t* radices);
+
 /* Reference state + init_problem! (src/simulation.jl:129-156, 305-312): builds the
  * Green's functions and spectral factors, the reference state, and performs the
  * first RHS evaluation (which forces the sparse update). */

@@ -269,3 +269,27 @@ def test_executors_bitwise_identical(monkeypatch, shape):
         for var in ("u", "ue", "dudt", "dz_ss"):
             for a, b in zip(base[var], out[var]):
                 assert np.array_equal(a, b), (ex, var)
+
+
+@pytest.mark.parametrize("form", FORMS)
+@pytest.mark.parametrize("case", ["config2_n350", "config5_n1024"])
+def test_rhs_parity_benchmark_sizes(form, case):
+    """One right-hand side at the benchmark grids (N = 350 glacial cycle, N = 1024 high
+    resolution, every channel on) against the oracle, at stage times inside and across
+    the sparse-update gate."""
+    sim = W.config2(form=form, N=350) if case == "config2_n350" else W.config5(form=form)
+    ref = pair(sim)
+    N = sim.domain.nx
+    rng = np.random.default_rng(N)
+    u = -80 * np.exp(-sim.domain.R**2 / (2 * (0.3 * sim.domain.Wx) ** 2)) + 0.2 * rng.standard_normal((N, N))
+    for t in (20e3, 20e3 + 12.5):
+        ug, dg = u.copy(), np.zeros_like(u)
+        F.update_diagnostics(dg, ug, sim, t)
+        ur, dr = ref.rhs(t, F_(u))
+        assert rel_l2(F_(ug), ur) < 1e-12
+        assert rel_l2(F_(dg), dr) < TOL[form], (case, t, rel_l2(F_(dg), dr))
+        assert rel_l2(F_(sim.get_field("ue")), ref.get_field(abi.FIELDS["ue"])) < TOL[form]
+        assert rel_l2(F_(sim.get_field("dz_ss")), ref.get_field(abi.FIELDS["dz_ss"])) < TOL[form]
+        u = u + 0.1 * dg
+    sim.close()
+    ref.close()

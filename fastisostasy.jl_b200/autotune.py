@@ -10,7 +10,7 @@ records the fastest per workload key in a JSON table shipped with the package
 
 The transforms (row and column FFTs of length N, padded convolutions of length M) run
 Stockham passes in a radix order; ``fft`` measures candidate orders of each length's
-factors (radices 2, 3, 4, 5, 7, 8, 16) per BS3 step of the single-simulation workload
+factors (radices 2, 3, 4, 5, 7, 8) per BS3 step of the single-simulation workload
 at that N and records the fastest as "fft:<L>"; ``fft_schedule_for`` reads it back and
 ``Simulation`` applies it through fi_set_fft_schedule.
 
@@ -59,14 +59,15 @@ def tiles_for(key):
 
 
 def fft_schedule_for(L):
-    """The tuned radix order for transforms of length L, or None."""
-    if os.environ.get("FI_NO_TUNING") == "1":
+    """The tuned radix order for transforms of length L, or None (FI_NO_TUNING=1 or
+    FI_NO_FFT_TUNING=1: the library's default order)."""
+    if os.environ.get("FI_NO_TUNING") == "1" or os.environ.get("FI_NO_FFT_TUNING") == "1":
         return None
     v = _load().get(f"fft:{L}")
     return list(v["schedule"]) if v else None
 
 
-REG_RADICES = (16, 8, 7, 5, 4, 3, 2)
+REG_RADICES = (8, 7, 5, 4, 3, 2)
 
 
 def default_schedule(L):

@@ -1,7 +1,7 @@
 // fi_fft.cuh -- shared-memory mixed-radix FFT for sm_100a.
 //
 // Batched 1D complex transforms staged in shared memory: Stockham autosort
-// passes (natural order in and out) with radix-2/3/4/5/7/8/16 butterflies held in
+// passes (natural order in and out) with radix-2/3/4/5/7/8 butterflies held in
 // registers and a generic odd-radix pass for any other prime factor.  These
 // replace the FFTW/CUFFT plans of the reference (src/tools.jl:100-108,
 // src/convolutions.jl:229-244).  Twiddles come from a per-length FP64 table
@@ -170,43 +170,6 @@ template <bool INV, typename T> struct SmallDft<8, INV, T> {
     }
 };
 
-// radix 16 as 4 x 4: DFT-4 over n1 of v[4 n1 + n2], twiddle w16^(n2 k1), DFT-4 over n2;
-// output k = k1 + 4 k2
-template <bool INV, typename T> struct SmallDft<16, INV, T> {
-    using C = cplx<T>;
-    static __device__ __forceinline__ void run(C* v) {
-        // cos / sin (2 pi m / 16), m = 0..9
-        const T cs[10] = {T(1), T(0.92387953251128675612818318939679), T(0.70710678118654752440084436210485),
-                          T(0.38268343236508977172845998403040), T(0), T(-0.38268343236508977172845998403040),
-                          T(-0.70710678118654752440084436210485), T(-0.92387953251128675612818318939679), T(-1),
-                          T(-0.92387953251128675612818318939679)};
-        const T sn[10] = {T(0), T(0.38268343236508977172845998403040), T(0.70710678118654752440084436210485),
-                          T(0.92387953251128675612818318939679), T(1), T(0.92387953251128675612818318939679),
-                          T(0.70710678118654752440084436210485), T(0.38268343236508977172845998403040), T(0),
-                          T(-0.38268343236508977172845998403040)};
-        C a[4][4];  // a[n2][k1]
-#pragma unroll
-        for (int n2 = 0; n2 < 4; n2++) {
-            C t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
-            SmallDft<4, INV, T>::run(t);
-#pragma unroll
-            for (int k1 = 0; k1 < 4; k1++) {
-                const int m = n2 * k1;  // 0..9
-                // forward twiddle exp(-2 pi i m / 16) = (cos, -sin); inverse conjugates it
-                const T wr = cs[m], wi = INV ? sn[m] : -sn[m];
-                a[n2][k1] = m == 0 ? t[k1] : cmk<C>(t[k1].x * wr - t[k1].y * wi, t[k1].x * wi + t[k1].y * wr);
-            }
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < 4; k1++) {
-            C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
-            SmallDft<4, INV, T>::run(t);
-#pragma unroll
-            for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[k2];
-        }
-    }
-};
-
 // ---------------------------------------------------------------------------
 // Stockham pass: nbatch transforms of length L at src[b*bstride + i]
 // ---------------------------------------------------------------------------
@@ -293,7 +256,6 @@ __device__ cplx<T>* fft_batch(cplx<T>* buf0, cplx<T>* buf1, const FftPlan& p, in
             case 5: stockham_pass<5, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
             case 7: stockham_pass<7, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
             case 8: stockham_pass<8, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
-            case 16: stockham_pass<16, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
             default: stockham_pass_generic<INV, T>(src, dst, tw, p.L, R, Ns, nbatch, bstride, tid, nth); break;
         }
         __syncthreads();

@@ -184,7 +184,7 @@ int fi_set_tiles(fi_handle* h, int32_t h_rows, int32_t B_cols);
 /* No counterpart in the reference (which calls FFTW/CUFFT plans): the radix schedule of
  * the library's transforms of length L (nx, ny or the padded convolution lengths Mx,
  * My), between fi_create and fi_init.  radices[0..n) are the Stockham passes in order;
- * they must multiply to L.  Radices 2, 3, 4, 5, 7, 8 and 16 run register butterflies,
+ * they must multiply to L.  Radices 2, 3, 4, 5, 7 and 8 run register butterflies,
  * any other factor a generic O(R^2) pass.  The default is radix 8 while possible, then
  * 4, 2, 7, 5, 3.  fastiso_b200.autotune measures schedules.  Results agree to rounding
  * across schedules.  fi_get_fft_schedule writes the current one (at most 20 passes). */

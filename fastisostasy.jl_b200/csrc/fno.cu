@@ -75,9 +75,18 @@ inline Offsets offsets() {
 // ---------------------------------------------------------------------------
 // device helpers
 // ---------------------------------------------------------------------------
+// GELU(a) = a Phi(a), Phi the standard normal distribution function
 __device__ __forceinline__ float gelu(float a) { return 0.5f * a * (1.f + erff(a * 0.70710678118654752f)); }
+// GELU and GELU'(a) = Phi(a) + a phi(a), Phi evaluated once
+__device__ __forceinline__ void gelu_both(float a, float& g, float& gp) {
+    const float Phi = 0.5f * (1.f + erff(a * 0.70710678118654752f));
+    g = a * Phi;
+    gp = Phi + a * 0.39894228040143268f * expf(-0.5f * a * a);
+}
 __device__ __forceinline__ float gelu_grad(float a) {
-    return 0.5f * (1.f + erff(a * 0.70710678118654752f)) + a * 0.39894228040143268f * expf(-0.5f * a * a);
+    float g, gp;
+    gelu_both(a, g, gp);
+    return gp;
 }
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -263,11 +272,11 @@ struct EpiProjBwd {
 #pragma unroll
         for (int i = 0; i < 16; i++) {
             const float a = v[i] + b1[j0 + i];
-            // Phi(a) once for GELU(a) = a Phi(a) and GELU'(a) = Phi(a) + a phi(a)
-            const float Phi = 0.5f * (1.f + erff(a * 0.70710678118654752f));
-            d[i] = g * Q2[j0 + i] * (Phi + a * 0.39894228040143268f * expf(-0.5f * a * a));
+            float ga, gpa;
+            gelu_both(a, ga, gpa);
+            d[i] = g * Q2[j0 + i] * gpa;
             t[(size_t)i * S2] = __float2bfloat16_rn(d[i]);
-            t[(size_t)(PW + i) * S2] = __float2bfloat16_rn(a * Phi);
+            t[(size_t)(PW + i) * S2] = __float2bfloat16_rn(ga);
         }
         store16(da_rows + (size_t)row * PW + j0, d);
     }

@@ -170,31 +170,41 @@ __device__ __forceinline__ void cp_async_wait() {
 template <int ROWS>
 __device__ __forceinline__ void tc_stage(uint32_t dst, const TcOperand& o1, const TcOperand& o2, int z1, int z2,
                                          int row0, int nrows, int k0, int K, int K1, const void* safe) {
-    // K-major groups: one 16-byte copy = 8 consecutive K elements of one row
-    for (int v = threadIdx.x; v < ROWS * 8; v += TC_THREADS) {
-        const int r = v >> 3, kv = v & 7;
-        const int gk = k0 + kv * 8;
+    static_assert(TC_THREADS % 8 == 0, "a thread keeps one K group of the K-major copies");
+    // K-major groups: one 16-byte copy = 8 consecutive K elements of one row; thread t
+    // always copies K group t % 8, so its operand and column are fixed
+    if (!(o1.mn && o2.mn)) {
+        const int kv = threadIdx.x & 7, gk = k0 + kv * 8;
         const bool second = gk >= K1;
         const TcOperand& o = second ? o2 : o1;
-        if (o.mn) continue;
-        const int gr = row0 + r, ck = second ? gk - K1 : gk;
-        const bool ok = gr < nrows && gk < K;
-        const void* src = ok ? (const void*)(o.p + (size_t)z1 * o.s + (size_t)z2 * o.s2 + (size_t)gr * o.ld + ck) : safe;
-        cp_async16(dst + tc_operand_offset(ROWS, r, kv * 8), src, ok);
+        if (!o.mn) {
+            const bool kok = gk < K;
+            const __nv_bfloat16* base =
+                kok ? o.p + (size_t)z1 * o.s + (size_t)z2 * o.s2 + (second ? gk - K1 : gk) : nullptr;
+            for (int r = threadIdx.x >> 3; r < ROWS; r += TC_THREADS / 8) {
+                const int gr = row0 + r;
+                const bool ok = kok && gr < nrows;
+                cp_async16(dst + tc_operand_offset(ROWS, r, kv * 8),
+                           ok ? (const void*)(base + (size_t)gr * o.ld) : safe, ok);
+            }
+        }
     }
     // MN-major groups: one 16-byte copy = 8 consecutive rows of one K column, stored as
     // row (k % 8) of core matrix (k / 8, r / 8)
-    constexpr int RV = ROWS / 8;
-    for (int v = threadIdx.x; v < RV * 64; v += TC_THREADS) {
-        const int kc = v / RV, rv = v - kc * RV;
-        const int gk = k0 + kc;
-        const bool second = gk >= K1;
-        const TcOperand& o = second ? o2 : o1;
-        if (!o.mn) continue;
-        const int gr = row0 + rv * 8, ck = second ? gk - K1 : gk;
-        const bool ok = gr < nrows && gk < K;
-        const void* src = ok ? (const void*)(o.p + (size_t)z1 * o.s + (size_t)z2 * o.s2 + (size_t)ck * o.ld + gr) : safe;
-        cp_async16(dst + (kc >> 3) * (ROWS * 16) + rv * 128 + (kc & 7) * 16, src, ok);
+    if (o1.mn || o2.mn) {
+        constexpr int RV = ROWS / 8;
+        for (int v = threadIdx.x; v < RV * 64; v += TC_THREADS) {
+            const int kc = v / RV, rv = v - kc * RV;
+            const int gk = k0 + kc;
+            const bool second = gk >= K1;
+            const TcOperand& o = second ? o2 : o1;
+            if (!o.mn) continue;
+            const int gr = row0 + rv * 8, ck = second ? gk - K1 : gk;
+            const bool ok = gr < nrows && gk < K;
+            const void* src =
+                ok ? (const void*)(o.p + (size_t)z1 * o.s + (size_t)z2 * o.s2 + (size_t)ck * o.ld + gr) : safe;
+            cp_async16(dst + (kc >> 3) * (ROWS * 16) + rv * 128 + (kc & 7) * 16, src, ok);
+        }
     }
 }
 

@@ -257,12 +257,15 @@ def ensemble_bench(dev, rank=0, world=1):
             "peak": peak, "peak_kind": kind, "unit": "GB/s",
             "frac": round(achieved / peak, 4) if achieved else None, "bytes_per_window": byts,
             "member_attempts": int(sum(sum(p.get("attempts", [])) for p in parts))}
-    from fastiso_b200.autotune import tiles_for
+    from fastiso_b200.autotune import ensemble_rule_for, tiles_for
 
+    rule = ensemble_rule_for()
+    tiles = (f"per member: h = B = clamp({rule} // N, 2, 16)" if rule is not None else
+             list(tiles_for(f"ensemble:{len(parts[0]['members'])}") or F.Ensemble.DEFAULT_TILES))
     return {"value": v, "unit": "member-kyr/s", "members": ENS_MEMBERS, "ranks": world,
             "members_per_rank": [len(p["members"]) for p in parts],
             "window": f"{ENS_WINDOW_YR:g} yr after 50 yr (of config 3's 20 kyr)",
-            "tiles": list(tiles_for(f"ensemble:{len(parts[0]['members'])}") or F.Ensemble.DEFAULT_TILES),
+            "tiles": tiles,
             "status_ok": ok, "ms": ms,
             "plain_fp64_loop": {"value": plain, "unit": "member-kyr/s",
                                 "sample": "4 members x 200 yr after 50 yr, one after another"},

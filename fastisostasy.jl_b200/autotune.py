@@ -17,6 +17,10 @@ at that N and records the fastest as "fft:<L>"; ``fft_schedule_for`` reads it ba
     python fastisostasy.jl_b200/autotune.py single 350     # config-2 grid (persistent executor)
     python fastisostasy.jl_b200/autotune.py ensemble 128   # config-3 ensemble
     python fastisostasy.jl_b200/autotune.py fft 350        # radix order of the length-350 transforms
+    python fastisostasy.jl_b200/autotune.py ensemble-rule 128   # per-member tiles h = B = c / N
+
+Ensemble members of different N get different tiles under the per-member rule, so that a
+task (tile of one member) costs about the same whatever the member's grid.
 """
 from __future__ import annotations
 
@@ -56,6 +60,54 @@ def tiles_for(key):
         return None
     v = _load().get(key)
     return tuple(v["tiles"]) if v else None
+
+
+def ensemble_rule_for():
+    """The tuned per-member tile rule of ensembles, c: member of grid N gets h = B =
+    clamp(c // N, 2, 16) (tasks of similar size across members), or None."""
+    if os.environ.get("FI_NO_TUNING") == "1":
+        return None
+    v = _load().get("ensemble:per_n")
+    return int(v["c"]) if v else None
+
+
+def rule_tiles(c, N):
+    t = max(2, min(16, int(c) // int(N)))
+    return (t, t)
+
+
+def time_ensemble_rule(n_members, c, years=1000.0, warm=50.0):
+    """Device ms per simulated member-year of the config-3 ensemble with per-member tiles
+    h = B = clamp(c // N, 2, 16)."""
+    members, t_ice, mod = W.config3_members(n_members=n_members)
+    sims = [W.config3_simulation(m, t_ice, mod, form="fp32") for m in members]
+    for s, m in zip(sims, members):
+        s.cfg.max_steps = 50_000_000
+        s.tiles = rule_tiles(c, m["N"])
+    ens = M.Ensemble(sims, tiles=None)
+    ens.step(warm)
+    ens.step(years)
+    ms = ens.last_gpu_ms / (years * n_members)
+    ens.close()
+    for s in sims:
+        s.close()
+    return ms
+
+
+def tune_ensemble_rule(n_members=128, candidates=(1024, 1536, 2048, 2560, 3072, 4096), write=True):
+    results = {}
+    for c in candidates:
+        results[c] = time_ensemble_rule(n_members, c)
+        print(json.dumps({"kind": "ensemble rule", "c": c, "ms_per_member_year": results[c]}), flush=True)
+    best = min(results, key=results.get)
+    entry = {"c": best, "ms_per_unit": results[best], "unit": "ms per simulated member-year (config 3, 1 kyr)",
+             "rule": "h = B = clamp(c // N, 2, 16)", "candidates": {str(k): v for k, v in results.items()}}
+    if write:
+        table = _load()
+        table["ensemble:per_n"] = entry
+        TABLE_DIR.mkdir(exist_ok=True)
+        TABLE.write_text(json.dumps(table, indent=1, sort_keys=True) + "\n")
+    return "ensemble:per_n", entry
 
 
 def fft_schedule_for(L):
@@ -205,5 +257,10 @@ def tune(kind, size, candidates=None, write=True):
 if __name__ == "__main__":
     kind = sys.argv[1] if len(sys.argv) > 1 else "single"
     size = int(sys.argv[2]) if len(sys.argv) > 2 else (128 if kind == "ensemble" else 350)
-    res = tune_fft(size) if kind == "fft" else tune(kind, size)
+    if kind == "fft":
+        res = tune_fft(size)
+    elif kind == "ensemble-rule":
+        res = tune_ensemble_rule(size)
+    else:
+        res = tune(kind, size)
     print(json.dumps(dict(zip(("key", "entry"), res))))

@@ -641,23 +641,31 @@ class Ensemble:
     that fails is reported in the returned status list and does not stop the others."""
 
     #: tile shape of members whose handles do not exist yet when the tuning table has
-    #: no entry: tall tiles, since the ensemble is throughput-bound
+    #: neither a per-member rule ("ensemble:per_n": h = B = c / N) nor an entry for this
+    #: ensemble size: tall tiles, since the ensemble is throughput-bound
     DEFAULT_TILES = (8, 8)
 
     def __init__(self, sims, tiles="auto"):
         self.sims = list(sims)
         if not self.sims:
             raise ValueError("an ensemble needs at least one member")
+        rule = None
         if isinstance(tiles, str):
-            from .autotune import tiles_for  # noqa: WPS433
+            from .autotune import ensemble_rule_for, tiles_for  # noqa: WPS433
 
+            rule = ensemble_rule_for()
             tiles = tiles_for(f"ensemble:{len(self.sims)}") or self.DEFAULT_TILES
         self.integrators = []
         for s in self.sims:
             if s.cfg.form != abi.FI_FORM_FP32:
                 raise UnsupportedError("ensemble members use the FP32 form")
-            if s._handle is None and s.tiles is None and tiles is not None:
-                s.tiles = tuple(tiles)
+            if s._handle is None and s.tiles is None:
+                if rule is not None:
+                    from .autotune import rule_tiles  # noqa: WPS433
+
+                    s.tiles = rule_tiles(rule, max(s.domain.nx, s.domain.ny))
+                elif tiles is not None:
+                    s.tiles = tuple(tiles)
             self.integrators.append(init_integrator(s))
         self.lib = self.sims[0].lib
         arr = (C.c_void_p * len(self.sims))(*[s._handle.value for s in self.sims])

@@ -235,6 +235,9 @@ _SIGS = {
     "fi_fno_train_step_weighted": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_float, C.POINTER(C.c_float)]),
     "fi_fno_adam": (C.c_int, [C.c_void_p, C.c_float]),
+    "fi_fno_loss_backward": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_float)]),
+    "fi_fno_grads_device": (C.c_void_p, [C.c_void_p]),
     "fi_fno_set_adam": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float]),
     "fi_fno_last_error": (C.c_char_p, [C.c_void_p]),
     "fi_fno_destroy": (None, [C.c_void_p]),

@@ -930,6 +930,21 @@ int fi_fno_train_step_weighted(fi_fno* h, int32_t B, const float* x, const float
     return rc;
 }
 
+int fi_fno_loss_backward(fi_fno* h, int32_t B, const float* x, const float* target, const float* w, float* loss) {
+    if (!h || !x || !target) return fail(h, FI_ERR_ARG, "null pointer");
+    int rc = check_batch(h, B);
+    if (rc) return rc;
+    FNO_CK(cudaSetDevice(h->device));
+    rc = forward(h, B, x, h->q);
+    if (!rc) rc = set_loss(h, B, target, w, nullptr);
+    if (!rc) rc = backward(h, B);
+    if (!rc) rc = finish(h);
+    if (!rc && loss) FNO_CK(cudaMemcpy(loss, h->scal, sizeof(float), cudaMemcpyDeviceToHost));
+    return rc;
+}
+
+void* fi_fno_grads_device(fi_fno* h) { return h ? (void*)h->grads : nullptr; }
+
 int fi_fno_adam(fi_fno* h, float lr) {
     if (!h) return FI_ERR_ARG;
     FNO_CK(cudaSetDevice(h->device));

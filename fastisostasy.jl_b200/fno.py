@@ -127,6 +127,32 @@ class FNO:
                     "fi_fno_train_step")
         return float(loss.value)
 
+    def loss_backward(self, x, target, weights=None) -> float:
+        """Forward, loss and backward without the optimizer step (data-parallel training:
+        reduce ``grads_tensor()`` across ranks, then ``adam``)."""
+        B = x.shape[0]
+        xp = self._tensor(x, (B, N_IN, self.S, self.S), "x")
+        tp = self._tensor(target, (B, self.S, self.S), "target")
+        wp = None if weights is None else self._tensor(weights, (B,), "weights")
+        loss = C.c_float(0.0)
+        self._sync_producer()
+        self._check(self._lib.fi_fno_loss_backward(self._h, B, xp, tp, wp, C.byref(loss)), "fi_fno_loss_backward")
+        return float(loss.value)
+
+    def grads_tensor(self):
+        """The gradient vector in device memory as a float32 torch tensor (no copy)."""
+        import torch
+
+        ptr = self._lib.fi_fno_grads_device(self._h)
+        if not ptr:
+            raise abi.FiError(abi.FI_ERR_ARG, "no gradient buffer")
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (self.n_params,), "typestr": "<f4", "data": (int(ptr), False),
+                                        "version": 3, "strides": None}
+
+        return torch.as_tensor(_View(), device=f"cuda:{self.device}")
+
     def adam(self, lr: float) -> None:
         self._check(self._lib.fi_fno_adam(self._h, C.c_float(lr)), "fi_fno_adam")
 

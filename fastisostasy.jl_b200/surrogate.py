@@ -163,14 +163,43 @@ class Dataset:
         return x, y
 
 
+def dp_step(net, x, y, w, lr, group=None):
+    """One training step, data-parallel when torch.distributed runs more than one rank:
+    the local forward, loss and backward (``net.loss_backward``), the gradient vector
+    averaged over the ranks in place (one all-reduce of num_params floats; NCCL over
+    NVLink on GPUs), then Adam on every rank.  Ranks that start from the same parameters
+    stay identical.  Returns the loss averaged over the ranks."""
+    import torch
+    import torch.distributed as dist
+
+    loss = net.loss_backward(x, y, w)
+    world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+    if world > 1:
+        g = net.grads_tensor()
+        dist.all_reduce(g, op=dist.ReduceOp.SUM, group=group)
+        g /= world
+        lt = torch.tensor([loss], dtype=torch.float32, device=g.device)
+        dist.all_reduce(lt, op=dist.ReduceOp.SUM, group=group)
+        loss = float(lt.item()) / world
+        if g.is_cuda:
+            torch.cuda.synchronize(g.device)  # the averaged gradients are in place before Adam
+    net.adam(lr)
+    return loss
+
+
 def train(net, data: Dataset, steps, batch=32, lr=1e-3, lr_min=1e-5, seed=0, log=None, log_every=500,
-          weighted=True):
+          weighted=True, group=None):
     """Adam with cosine decay on random (trajectory, macro-step) pairs, loss weighted per
     trajectory (``Dataset.w``) unless weighted=False; returns the loss history and the
-    measured training throughput (samples/s, including batch assembly)."""
+    measured training throughput (samples/s, including batch assembly).  Under
+    torch.distributed with several ranks every rank draws its own batches and the
+    gradients are averaged each step (``dp_step``); samples/s then counts all ranks."""
     import torch
+    import torch.distributed as dist
 
-    g = torch.Generator(device=data.u.device).manual_seed(seed)
+    world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
+    rank = dist.get_rank(group) if world > 1 else 0
+    g = torch.Generator(device=data.u.device).manual_seed(seed + 7919 * rank)
     hist = []
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -180,12 +209,15 @@ def train(net, data: Dataset, steps, batch=32, lr=1e-3, lr_min=1e-5, seed=0, log
         x, y = data.batch(traj, k)
         a = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * it / max(steps, 1)))
         w = data.w[traj].contiguous() if weighted else None
-        hist.append(net.train_step(x, y, float(a), weights=w))
+        if world > 1:
+            hist.append(dp_step(net, x, y, w, float(a), group))
+        else:
+            hist.append(net.train_step(x, y, float(a), weights=w))
         if log and (it + 1) % log_every == 0:
             log(f"step {it + 1}/{steps} loss {np.mean(hist[-log_every:]):.4e}")
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    return {"loss": hist, "samples_per_s": steps * batch / dt, "seconds": dt}
+    return {"loss": hist, "samples_per_s": world * steps * batch / dt, "seconds": dt, "ranks": world}
 
 
 def rollout(net, u0, static, n_steps):

@@ -314,6 +314,13 @@ int fi_fno_train_step(fi_fno* h, int32_t B, const float* x, const float* target,
 int fi_fno_train_step_weighted(fi_fno* h, int32_t B, const float* x, const float* target, const float* w,
                                float lr, float* loss);
 int fi_fno_adam(fi_fno* h, float lr); /* one Adam step with the current gradients */
+/* Data-parallel training: forward, loss and backward without the optimizer step, then
+ * the caller reduces the gradient vector (fi_fno_grads_device: num_params floats on the
+ * handle's device, valid for its lifetime) across ranks in place, e.g. an NCCL
+ * all-reduce averaged over the ranks, and calls fi_fno_adam on every rank.  Ranks that
+ * start from the same parameters stay identical. */
+int fi_fno_loss_backward(fi_fno* h, int32_t B, const float* x, const float* target, const float* w, float* loss);
+void* fi_fno_grads_device(fi_fno* h);
 int fi_fno_set_adam(fi_fno* h, float beta1, float beta2, float eps); /* default 0.9, 0.999, 1e-8 */
 const char* fi_fno_last_error(const fi_fno* h);
 void fi_fno_destroy(fi_fno* h);

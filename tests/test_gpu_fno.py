@@ -141,3 +141,31 @@ def test_batch_limits(torch):
         net.backward(torch.zeros((2, 32, 32), device="cuda"))  # the last chunk had B = 1
     net.backward(torch.zeros((1, 32, 32), device="cuda"))
     net.close()
+
+
+def test_split_step_matches_train_step(torch):
+    """loss_backward + adam (the data-parallel split) is train_step, and grads_tensor is a
+    zero-copy view of the gradient vector."""
+    S, B = 32, 4
+    a, p = _net(S, B, seed=31)
+    b, _ = _net(S, B, seed=31)
+    rng = np.random.default_rng(12)
+    x = torch.from_numpy(rng.standard_normal((B, 6, S, S)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((B, S, S)).astype(np.float32)).cuda()
+    w = torch.tensor([1.0, 0.5, 2.0, 1.5], device="cuda")
+    la = a.train_step(x, t, 1e-3, weights=w)
+    lb = b.loss_backward(x, t, weights=w)
+    g = b.grads_tensor()
+    assert g.shape == (b.n_params,) and g.is_cuda
+    np.testing.assert_array_equal(g.cpu().numpy(), b.get_grads())
+    b.adam(1e-3)
+    assert abs(la - lb) <= 1e-6 * abs(la)
+    pa, pb = a.get_params(), b.get_params()
+    assert _rel(pb, pa.astype(np.float64)) < 1e-6
+    from fastiso_b200.surrogate import dp_step
+
+    dp_step(b, x, t, w, 1e-3)          # one rank: no collective, the same update
+    a.train_step(x, t, 1e-3, weights=w)
+    assert _rel(b.get_params(), a.get_params().astype(np.float64)) < 1e-6
+    a.close()
+    b.close()

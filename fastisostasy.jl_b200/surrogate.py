@@ -1,5 +1,5 @@
 """Surrogate of a 100-yr macro-step of the LV-ELVA solver, and the screening loop in which
-the plain solver judges its proposals.  No counterpart in FastIsostasy.jl (its closest
+the plain solver checks its proposals.  No counterpart in FastIsostasy.jl (its closest
 precedent is the threaded ensemble of ext/FastIsostasyEnsembleKalmanProcessesExt.jl:107-122,
 which runs the solver for every candidate).
 
@@ -286,7 +286,7 @@ class ScreenReport:
     misfit_rejects: int
     surrogate_seconds: float
     solver_seconds: float
-    judged: list = field(default_factory=list)   # (pool index, surrogate error, solver misfit, accepted)
+    checked: list = field(default_factory=list)   # (pool index, surrogate error, solver misfit, accepted)
 
 
 def solve_final(specs, t_end, batch=128):
@@ -311,8 +311,8 @@ def _misfit(u, obs):
     return float(np.linalg.norm(u - obs) / max(np.linalg.norm(obs), 1e-30))
 
 
-def screen(net, pool, obs, n_accept, tol_obs, bound, t_end, judge_batch=8, solver=None):
-    """Surrogate proposes, plain solver judges.  pool: MemberSpecs; obs: observed u(t_end)
+def screen(net, pool, obs, n_accept, tol_obs, bound, t_end, solve_batch=8, solver=None, device="cuda"):
+    """Surrogate proposes, plain solver checks.  pool: MemberSpecs; obs: observed u(t_end)
     [N, N].  A proposal is accepted when the solver's u(t_end) fits obs within tol_obs
     (rel-L2) and the surrogate's prediction is within `bound` (rel-L2) of the solver's;
     otherwise it is replaced by the next proposal.  solver(specs, t_end) -> u(t_end)
@@ -321,15 +321,15 @@ def screen(net, pool, obs, n_accept, tol_obs, bound, t_end, judge_batch=8, solve
 
     solver = solver or solve_final
     t0 = time.perf_counter()
-    static = torch.from_numpy(np.stack([static_features(s) for s in pool])).cuda()
-    u0 = torch.zeros((len(pool), pool[0].N, pool[0].N), device="cuda")
+    static = torch.from_numpy(np.stack([static_features(s) for s in pool])).to(device)
+    u0 = torch.zeros((len(pool), pool[0].N, pool[0].N), device=device)
     pred = rollout(net, u0, static, int(round(t_end / MACRO_DT)))[-1].cpu().numpy()
     t_sur = time.perf_counter() - t0
     order = np.argsort([_misfit(p, obs) for p in pred])
     rep = ScreenReport([], 0, 0, 0, t_sur, 0.0)
     pos = 0
     while len(rep.accepted) < n_accept and pos < len(order):
-        take = order[pos:pos + min(judge_batch, n_accept - len(rep.accepted))]
+        take = order[pos:pos + min(solve_batch, n_accept - len(rep.accepted))]
         pos += len(take)
         t1 = time.perf_counter()
         exact = solver([pool[i] for i in take], t_end)
@@ -344,18 +344,18 @@ def screen(net, pool, obs, n_accept, tol_obs, bound, t_end, judge_batch=8, solve
                 rep.misfit_rejects += 1
             if ok:
                 rep.accepted.append((int(i), u))
-            rep.judged.append((int(i), e, m, ok))
+            rep.checked.append((int(i), e, m, ok))
     return rep
 
 
-def screen_without_surrogate(pool, obs, n_accept, tol_obs, t_end, seed=0, judge_batch=8, solver=None):
+def screen_without_surrogate(pool, obs, n_accept, tol_obs, t_end, seed=0, solve_batch=8, solver=None):
     """The same acceptance loop with the solver alone: candidates in random order."""
     solver = solver or solve_final
     order = np.random.default_rng(seed).permutation(len(pool))
     rep = ScreenReport([], 0, 0, 0, 0.0, 0.0)
     pos = 0
     while len(rep.accepted) < n_accept and pos < len(order):
-        take = order[pos:pos + min(judge_batch, n_accept - len(rep.accepted))]
+        take = order[pos:pos + min(solve_batch, n_accept - len(rep.accepted))]
         pos += len(take)
         t1 = time.perf_counter()
         exact = solver([pool[i] for i in take], t_end)
@@ -367,7 +367,7 @@ def screen_without_surrogate(pool, obs, n_accept, tol_obs, t_end, seed=0, judge_
                 rep.accepted.append((int(i), u))
             else:
                 rep.misfit_rejects += 1
-            rep.judged.append((int(i), None, m, m <= tol_obs))
+            rep.checked.append((int(i), None, m, m <= tol_obs))
     return rep
 
 
@@ -444,8 +444,8 @@ def main(argv=None):
     exact = solve_final(pool, a.t_end)
     t_all = time.perf_counter() - t1
     mis = np.array([_misfit(x, obs) for x in exact])
-    ws = screen(net, pool, obs, a.accept, a.tol, a.bound, a.t_end, judge_batch=a.accept)
-    wo = screen_without_surrogate(pool, obs, a.accept, a.tol, a.t_end, seed=1, judge_batch=a.accept)
+    ws = screen(net, pool, obs, a.accept, a.tol, a.bound, a.t_end, solve_batch=a.accept)
+    wo = screen_without_surrogate(pool, obs, a.accept, a.tol, a.t_end, seed=1, solve_batch=a.accept)
     rep["screening"] = {
         "pool": a.pool, "qualifying_in_pool": int((mis <= a.tol).sum()), "tol": a.tol, "bound": a.bound,
         "solver_all_pool_seconds": t_all,
@@ -453,12 +453,12 @@ def main(argv=None):
                            "out_of_bound": ws.out_of_bound, "misfit_rejects": ws.misfit_rejects,
                            "surrogate_seconds": ws.surrogate_seconds, "solver_seconds": ws.solver_seconds,
                            "accepted_solver_misfit_max": max([_misfit(u, obs) for _, u in ws.accepted], default=None),
-                           "judged": [(i, e, m, ok) for i, e, m, ok in ws.judged]},
+                           "checked": [(i, e, m, ok) for i, e, m, ok in ws.checked]},
         "without_surrogate": {"solver_runs": wo.solver_runs, "accepted": len(wo.accepted),
                               "solver_seconds": wo.solver_seconds},
     }
     log(json.dumps({k: v for k, v in rep["screening"].items() if k not in ("with_surrogate",)}))
-    log(json.dumps({k: v for k, v in rep["screening"]["with_surrogate"].items() if k != "judged"}))
+    log(json.dumps({k: v for k, v in rep["screening"]["with_surrogate"].items() if k != "checked"}))
     with open(a.out, "w") as f:
         json.dump(rep, f, indent=1)
     net.close()

@@ -1,6 +1,6 @@
 """The surrogate end to end at a reduced size: trajectories from the GPU solver, training
 with the FNO's own CUDA kernels, held-out accuracy, and screening in which the plain
-solver judges the surrogate's proposals -- against the same screening without it."""
+solver checks the surrogate's proposals -- against the same screening without it."""
 import numpy as np
 import pytest
 
@@ -43,9 +43,9 @@ def test_screening_gain(trained):
     truth, pool = S.calibration_pool(96, N, W, seed=777)
     obs = S.solve_final([truth], T_END)[0]
     tol, bound = 0.06, 0.15
-    with_s = S.screen(net, pool, obs, n_accept=3, tol_obs=tol, bound=bound, t_end=T_END, judge_batch=3)
-    without = S.screen_without_surrogate(pool, obs, n_accept=3, tol_obs=tol, t_end=T_END, seed=1, judge_batch=3)
+    with_s = S.screen(net, pool, obs, n_accept=3, tol_obs=tol, bound=bound, t_end=T_END, solve_batch=3)
+    without = S.screen_without_surrogate(pool, obs, n_accept=3, tol_obs=tol, t_end=T_END, seed=1, solve_batch=3)
     assert len(with_s.accepted) == 3 and len(without.accepted) == 3
     for _, u in with_s.accepted:     # accepted members carry the solver's own states
         assert S._misfit(u, obs) <= tol
-    assert with_s.solver_runs < without.solver_runs, (with_s.solver_runs, without.solver_runs, with_s.judged)
+    assert with_s.solver_runs < without.solver_runs, (with_s.solver_runs, without.solver_runs, with_s.checked)

@@ -97,6 +97,7 @@ struct fi_handle {
     unsigned int* d_bar = nullptr;
     PersistArgs pargs{};
     int persist_grid = 0;
+    int persist_minb = 2;  // which k_persist build runs (blocks per SM of its register budget)
     size_t persist_smem = 0;
     unsigned long long* d_trace = nullptr;  // phase timeline of the persistent executor
     // plain form
@@ -1366,8 +1367,18 @@ static int setup_persist(fi_handle* h, int K) {
         h->executor = EXEC_GRAPH;
         return FI_OK;
     }
+    // the 2-blocks-per-SM build where shared memory fits two blocks, else the one sized
+    // for a single block (more registers, no spills); FI_PERSIST_MINB=1|2 forces one
     CK(cudaFuncSetAttribute(k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaFuncSetAttribute(k_persist1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persist, ROW_THREADS, smem));
+    h->persist_minb = occ >= 2 ? 2 : 1;
+    const char* mb = getenv("FI_PERSIST_MINB");
+    if (mb && (mb[0] == '1' || mb[0] == '2')) h->persist_minb = mb[0] - '0';
+    if (h->persist_minb == 1) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persist1, ROW_THREADS, smem));
+        occ = std::min(occ, 1);
+    }
     if (occ < 1) {
         h->executor = EXEC_GRAPH;
         return FI_OK;
@@ -1380,7 +1391,8 @@ static int setup_persist(fi_handle* h, int K) {
 static int run_segment_persist(fi_handle* h) {
     CK(cudaMemsetAsync(h->d_bar, 0, 4 * sizeof(unsigned int), h->stream));
     void* args[] = {(void*)&h->pargs};
-    CK(cudaLaunchCooperativeKernel((const void*)k_persist, dim3(h->persist_grid), dim3(ROW_THREADS), args,
+    const void* kfn = h->persist_minb == 1 ? (const void*)k_persist1 : (const void*)k_persist;
+    CK(cudaLaunchCooperativeKernel(kfn, dim3(h->persist_grid), dim3(ROW_THREADS), args,
                                    h->persist_smem, h->stream));
     unsigned int bar[4];
     CK(cudaMemcpyAsync(bar, h->d_bar, sizeof(bar), cudaMemcpyDeviceToHost, h->stream));

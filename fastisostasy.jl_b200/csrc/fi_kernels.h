@@ -48,7 +48,8 @@ enum {
     PH_ROWS_FWD2, PH_COLS2, PH_ROWS_FWD3, PH_COLS3, PH_ROWS_FWD4, PH_COLS4, PH_ROWS_INV4, PH_CONTROLLER,
     PH_COUNT
 };
-__global__ void k_persist(PersistArgs a);
+__global__ void k_persist(PersistArgs a);   // two blocks per SM
+__global__ void k_persist1(PersistArgs a);  // one block per SM (larger register budget)
 // fills the shared-memory layout fields of a and returns the dynamic shared memory bytes
 size_t persist_layout(int nx, int ny, int Mx, int My, int K, int fwd_bytes, int h_rows, int ncols, int B_cols,
                       int h_conv, int B_conv, PersistArgs* a);

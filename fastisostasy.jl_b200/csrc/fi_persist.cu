@@ -25,7 +25,10 @@
 
 namespace fi {
 
-__global__ void __launch_bounds__(RT, 2) k_persist(PersistArgs a) {
+// The executor body, inlined into two kernels whose register budgets differ: k_persist
+// for two blocks per SM (64 registers a thread) where shared memory fits two blocks,
+// k_persist1 for one (no spills) where it fits only one.
+__device__ __forceinline__ void persist_body(const PersistArgs& a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Member sm;
     __shared__ Ctl sc;
@@ -223,5 +226,8 @@ size_t persist_layout(int nx, int ny, int Mx, int My, int K, int fwd_bytes, int 
     a->tice_off = (K <= TICE_MAX) ? ntw : -1;
     return ws + (size_t)ntw * sizeof(float2) + (K <= TICE_MAX ? (size_t)K * sizeof(double) : 0);
 }
+
+__global__ void __launch_bounds__(RT, 2) k_persist(PersistArgs a) { persist_body(a); }
+__global__ void __launch_bounds__(RT, 1) k_persist1(PersistArgs a) { persist_body(a); }
 
 }  // namespace fi

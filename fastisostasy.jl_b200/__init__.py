@@ -5,6 +5,7 @@ BoundaryConditions, RegionalSeaLevel, Simulation, run!, init_integrator, step!,
 update_diagnostics!) over the C ABI of libfastiso_b200.so (include/fastiso_b200.h).
 """
 from . import abi  # noqa: F401
+from .fno import FNO  # noqa: F401  (the surrogate network; its workflow is fastiso_b200.surrogate)
 from .model import (  # noqa: F401
     BoundaryConditions, CompressibleLithosphereColumn, CompressibleMantle, ConstantBSL, CornerBC, DiffEqOptions, Ensemble,
     ExtendedBCSpace, ExternallyUpdatedIceThickness, FreqDomainViscosityLumping, IncompressibleLithosphereColumn,

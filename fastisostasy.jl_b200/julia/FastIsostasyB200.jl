@@ -62,12 +62,14 @@ function getfield_b200(b::B200Simulation, id::Integer)
 end
 
 """
-    B200Simulation(sim, t_span; form = :fp32, device = 0)
+    B200Simulation(sim, t_span; form = :fp32, device = 0, tiles = nothing, fft_schedules = Dict())
 
 A GPU twin of `sim` (laterally-variable ELVA with Maxwell mantle) over `t_span`, the
-same tuple given to `Simulation`: the same inputs, run by libfastiso_b200.so.
+same tuple given to `Simulation`: the same inputs, run by libfastiso_b200.so.  `tiles =
+(h_rows, B_cols)` and `fft_schedules = Dict(L => [radices...])` pass tuned settings
+(fastiso_b200's `tuning/b200.json`) to fi_set_tiles / fi_set_fft_schedule.
 """
-function B200Simulation(sim, t_span; form = :fp32, device = 0)
+function B200Simulation(sim, t_span; form = :fp32, device = 0, tiles = nothing, fft_schedules = Dict())
     d, c, se, sl, bcs = sim.domain, sim.c, sim.solidearth, sim.sealevel, sim.bcs
     cfg = FiConfig()
     ccall((:fi_config_default, LIB), Cvoid, (Ref{FiConfig}, Int32, Int32, Float64, Float64), cfg, d.nx, d.ny,
@@ -92,6 +94,15 @@ function B200Simulation(sim, t_span; form = :fp32, device = 0)
     check(ccall((:fi_create, LIB), Cint, (Ref{FiConfig}, Ref{Ptr{Cvoid}}), cfg, h), C_NULL, "fi_create")
     b = B200Simulation(sim, h[])
     finalizer(x -> ccall((:fi_destroy, LIB), Cvoid, (Ptr{Cvoid},), x.h), b)
+    if tiles !== nothing && form == :fp32
+        check(ccall((:fi_set_tiles, LIB), Cint, (Ptr{Cvoid}, Int32, Int32), b.h, tiles[1], tiles[2]),
+              b.h, "fi_set_tiles")
+    end
+    for (L, r) in fft_schedules
+        rr = Vector{Int32}(r)
+        check(ccall((:fi_set_fft_schedule, LIB), Cint, (Ptr{Cvoid}, Int32, Int32, Ptr{Int32}),
+                    b.h, L, length(rr), rr), b.h, "fi_set_fft_schedule")
+    end
     set_field!(b, F.litho_rigidity, se.litho_rigidity)
     set_field!(b, F.effective_viscosity, se.effective_viscosity)
     set_field!(b, F.pseudodiff_scaling, se.pseudodiff_scaling)
@@ -141,5 +152,34 @@ step!(b::B200Simulation, dt::Real) =
 set_ice!(b::B200Simulation, H::AbstractMatrix) = set_field!(b, F.H_ice, H)
 
 current_u(b::B200Simulation) = getfield_b200(b, F.u)
+
+"""
+    B200Ensemble(members::Vector{B200Simulation})
+
+Members (FP32 form, each after init_integrator) advanced together by the persistent
+ensemble kernel; `step!(e, dt)` is step!(integrator_m, dt, true) for every member and
+returns the members' status codes (a failing member does not stop the others).
+"""
+mutable struct B200Ensemble
+    members::Vector{B200Simulation}
+    h::Ptr{Cvoid}
+end
+
+function B200Ensemble(members::Vector{B200Simulation})
+    hs = [m.h for m in members]
+    e = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:fi_ensemble_create, LIB), Cint, (Ptr{Ptr{Cvoid}}, Int32, Ref{Ptr{Cvoid}}), hs, length(hs), e)
+    rc == 0 || error("fi_ensemble_create failed ($rc)")
+    ens = B200Ensemble(members, e[])
+    finalizer(x -> ccall((:fi_ensemble_destroy, LIB), Cvoid, (Ptr{Cvoid},), x.h), ens)
+    return ens
+end
+
+function step!(e::B200Ensemble, dt::Real)
+    status = zeros(Int32, length(e.members))
+    rc = ccall((:fi_ensemble_step, LIB), Cint, (Ptr{Cvoid}, Float64, Ptr{Int32}), e.h, dt, status)
+    rc == 0 || error("fi_ensemble_step failed ($rc)")
+    return status
+end
 
 end  # module

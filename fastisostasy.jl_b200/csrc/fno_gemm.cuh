@@ -22,6 +22,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "../../include/fastiso_b200.h"
 
@@ -338,15 +339,15 @@ struct EpiStoreF32 {
 template <int BN, class Epi>
 inline cudaError_t launch_gemm_tc(const TcGemmArgs& g, int batch, const Epi& epi, cudaStream_t st) {
     constexpr int STAGE = (TC_BM + BN) * TC_BK * 2;
-    static unsigned attr_set = 0;  // one bit per device
+    static std::atomic<unsigned> attr_set{0};  // one bit per device (handles may run on several threads)
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= 32) return cudaErrorInvalidDevice;
-    if (!(attr_set & (1u << dev))) {
+    if (!(attr_set.load() & (1u << dev))) {
         e = cudaFuncSetAttribute(k_gemm_tc<BN, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * STAGE);
         if (e != cudaSuccess) return e;
-        attr_set |= 1u << dev;
+        attr_set.fetch_or(1u << dev);
     }
     TcGemmArgs a = g;
     a.batch = batch;

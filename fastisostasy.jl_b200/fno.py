@@ -140,7 +140,8 @@ class FNO:
         return float(loss.value)
 
     def grads_tensor(self):
-        """The gradient vector in device memory as a float32 torch tensor (no copy)."""
+        """The gradient vector in device memory as a float32 torch tensor (no copy; valid
+        while this handle is open, rewritten by the next backward pass)."""
         import torch
 
         ptr = self._lib.fi_fno_grads_device(self._h)

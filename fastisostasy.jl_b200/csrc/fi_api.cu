@@ -1847,7 +1847,7 @@ static int ensemble_step_persist(fi_ensemble* e, std::vector<std::vector<double>
             state[i] = 1;
             any = true;
         }
-        // members without a segment this round must not step: their t_stop is their t
+        // members without a segment in this ensemble step must not step: their t_stop is their t
         for (int i = 0; i < n; i++) {
             if (state[i] == 1) continue;
             fi_handle* h = e->mem[i];

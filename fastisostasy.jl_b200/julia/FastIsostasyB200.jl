@@ -4,7 +4,7 @@
 # prepare every input: rigidity, effective viscosity, R, masks, reference state, ice
 # history) and runs `run!` / `init_integrator` + `step!` semantics on the GPU.  Julia
 # matrices are column-major with dimension 1 = x, which is the C ABI's layout, so arrays
-# are passed without a transpose.  Not exercised here: this build environment has no Julia.
+# are passed without a transpose.  Not exercised by the test suite, which runs without Julia.
 module FastIsostasyB200
 
 using FastIsostasy

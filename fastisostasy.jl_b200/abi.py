@@ -41,6 +41,9 @@ FI_ICE_EXTERNAL = 1
 FI_EXEC_PERSIST = 0
 FI_EXEC_GRAPH = 1
 FI_EXEC_LOOP = 2
+FI_WAIT_GRID_POLLS = 0
+FI_WAIT_GRID_EXTRA_ARRIVALS = 1
+FI_WAIT_TC_POLLS = 2
 FI_NUM_PHASES = 11
 PHASE_NAMES = ("conv_rows", "conv_cols", "conv_rows_inv", "rows_fwd2", "cols2", "rows_fwd3", "cols3", "rows_fwd4",
                "cols4", "rows_inv4", "controller")
@@ -210,6 +213,9 @@ _SIGS = {
                          C.POINTER(C.c_double)]),
     "fi_init_integrator": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "fi_step": (C.c_int, [C.c_void_p, C.c_double]),
+    "fi_record_steps": (C.c_int, [C.c_void_p, C.c_int64]),
+    "fi_get_step_record": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.POINTER(C.c_int64)]),
+    "fi_set_step_replay": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]),
     "fi_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FiStats)]),
     "fi_checkpoint": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]),
     "fi_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
@@ -241,6 +247,7 @@ _SIGS = {
     "fi_fno_set_adam": (C.c_int, [C.c_void_p, C.c_float, C.c_float, C.c_float]),
     "fi_fno_last_error": (C.c_char_p, [C.c_void_p]),
     "fi_fno_destroy": (None, [C.c_void_p]),
+    "fi_debug_set_wait_limit": (C.c_int, [C.c_int32, C.c_int64]),
     "fi_last_error": (C.c_char_p, [C.c_void_p]),
     "fi_status_string": (C.c_char_p, [C.c_int32]),
     "fi_destroy": (None, [C.c_void_p]),

@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <string>
 #include <vector>
@@ -114,6 +115,10 @@ struct fi_handle {
     size_t smem_cap = 0;
     double last_rhs_t = 0.0;
     long long nf_plain = 0;
+    // step-sequence record / replay buffers (FP32 form: device, plain form: host)
+    double* d_rec = nullptr;
+    double* d_replay = nullptr;
+    std::vector<double> h_rec, h_replay;
 };
 
 static int set_err(fi_handle* h, int code, const char* fmt, ...) {
@@ -344,6 +349,8 @@ void fi_destroy(fi_handle* h) {
     if (h->seg_exec) cudaGraphExecDestroy(h->seg_exec);
     if (h->seg_graph) cudaGraphDestroy(h->seg_graph);
     for (void* p : h->allocs) cudaFree(p);
+    if (h->d_rec) cudaFree(h->d_rec);
+    if (h->d_replay) cudaFree(h->d_replay);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -1388,8 +1395,15 @@ static int setup_persist(fi_handle* h, int K) {
     return FI_OK;
 }
 
+// Wait bounds of the device waits (fi_debug_set_wait_limit): negative = the default.
+static std::atomic<long long> g_grid_polls{-1};
+static std::atomic<long long> g_grid_extra{0};
+
 static int run_segment_persist(fi_handle* h) {
     CK(cudaMemsetAsync(h->d_bar, 0, 4 * sizeof(unsigned int), h->stream));
+    const long long gp = g_grid_polls.load();
+    h->pargs.polls = gp >= 0 ? gp : PERSIST_SPIN_LIMIT;
+    h->pargs.bar_extra = (unsigned)g_grid_extra.load();
     void* args[] = {(void*)&h->pargs};
     const void* kfn = h->persist_minb == 1 ? (const void*)k_persist1 : (const void*)k_persist;
     CK(cudaLaunchCooperativeKernel(kfn, dim3(h->persist_grid), dim3(ROW_THREADS), args,
@@ -1656,6 +1670,95 @@ extern "C" int fi_step(fi_handle* h, double dt) {
     v.insert(v.end(), rest.begin(), rest.end());
     h->last_call = 0;
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// step-sequence record and replay: the controller (fi_device.cuh) appends every
+// accepted dt to ctl.rec_dt and, while a replay is installed, accepts every attempt
+// and takes the next dt from ctl.replay_dt.  FP32 form: device arrays (the control
+// block lives on the device); plain form: host arrays (host controller).
+// ---------------------------------------------------------------------------
+extern "C" int fi_record_steps(fi_handle* h, int64_t cap) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h || cap < 0) return FI_ERR_ARG;
+    if (!h->integ_started) return set_err(h, FI_ERR_STATE, "fi_init_integrator not called");
+    const bool fused = h->cfg.form == FI_FORM_FP32;
+    if (fused) RET(read_ctl(h));
+    if (h->d_rec) {
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaFree(h->d_rec));
+        h->d_rec = nullptr;
+    }
+    h->h_rec.clear();
+    h->h_rec.shrink_to_fit();
+    double* p = nullptr;
+    if (cap > 0) {
+        if (fused) {
+            CK(cudaMalloc(&h->d_rec, (size_t)cap * sizeof(double)));
+            p = h->d_rec;
+        } else {
+            h->h_rec.assign((size_t)cap, 0.0);
+            p = h->h_rec.data();
+        }
+    }
+    h->ctl.rec_dt = p;
+    h->ctl.rec_cap = cap;
+    h->ctl.rec_n = 0;
+    if (fused) RET(write_ctl(h));
+    return FI_OK;
+}
+
+extern "C" int fi_get_step_record(fi_handle* h, double* dts, int64_t cap, int64_t* n) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h || !n || cap < 0 || (cap > 0 && !dts)) return FI_ERR_ARG;
+    if (!h->integ_started) return set_err(h, FI_ERR_STATE, "fi_init_integrator not called");
+    if (h->cfg.form == FI_FORM_FP32) RET(read_ctl(h));
+    const long long stored = std::min(h->ctl.rec_n, h->ctl.rec_cap);
+    const long long k = std::min<long long>(stored, cap);
+    if (k > 0) {
+        if (h->cfg.form == FI_FORM_FP32) {
+            CK(cudaMemcpyAsync(dts, h->d_rec, (size_t)k * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        } else {
+            memcpy(dts, h->h_rec.data(), (size_t)k * sizeof(double));
+        }
+    }
+    *n = h->ctl.rec_n;
+    return FI_OK;
+}
+
+extern "C" int fi_set_step_replay(fi_handle* h, int64_t n, const double* dts) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h || n < 0 || (n > 0 && !dts)) return FI_ERR_ARG;
+    if (!h->integ_started) return set_err(h, FI_ERR_STATE, "fi_init_integrator not called");
+    for (int64_t i = 0; i < n; i++)
+        if (!(fabs(dts[i]) > 0 && fabs(dts[i]) < INFINITY))
+            return set_err(h, FI_ERR_ARG, "replayed dt[%lld] is zero or not finite", (long long)i);
+    const bool fused = h->cfg.form == FI_FORM_FP32;
+    if (fused) RET(read_ctl(h));
+    if (h->d_replay) {
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaFree(h->d_replay));
+        h->d_replay = nullptr;
+    }
+    h->h_replay.assign(dts, dts + n);
+    const double* p = nullptr;
+    if (n > 0) {
+        if (fused) {
+            CK(cudaMalloc(&h->d_replay, (size_t)n * sizeof(double)));
+            CK(cudaMemcpyAsync(h->d_replay, dts, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+            p = h->d_replay;
+        } else {
+            p = h->h_replay.data();
+        }
+        h->ctl.dt = fabs(dts[0]);
+        h->ctl.dtpropose = fabs(dts[0]);
+    }
+    h->ctl.replay_dt = p;
+    h->ctl.replay_n = n;
+    h->ctl.replay_i = n > 0 ? 1 : 0;
+    if (fused) RET(write_ctl(h));
+    return FI_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -2205,23 +2308,52 @@ static std::vector<Blob> state_blobs(fi_handle* h) {
     return b;
 }
 
+// Checkpoint layout: CkHeader, the control block, nf_plain, last_call, the tstops
+// (CkHeader::nts doubles), then the state blobs of the handle's form in order.
+struct CkHeader {
+    char magic[8];        // "FICKPT\0\0"
+    uint32_t version;     // CK_VERSION
+    int32_t form;         // FI_FORM_*
+    int32_t nx, ny;
+    uint32_t ctl_bytes;   // sizeof(Ctl)
+    uint32_t nblobs;
+    uint64_t nts;         // tstops
+    uint64_t total;       // bytes of the whole checkpoint
+};
+static const char CK_MAGIC[8] = {'F', 'I', 'C', 'K', 'P', 'T', 0, 0};
+constexpr uint32_t CK_VERSION = 2;
+
+static size_t ck_size(const std::vector<Blob>& blobs, size_t nts) {
+    size_t need = sizeof(CkHeader) + sizeof(Ctl) + sizeof(long long) + sizeof(int) + nts * sizeof(double);
+    for (auto& b : blobs) need += b.bytes;
+    return need;
+}
+
 extern "C" int fi_checkpoint(fi_handle* h, void* buf, size_t* size) {
     if (h) cudaSetDevice(h->cfg.device);
     if (!h || !size) return FI_ERR_ARG;
     if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init not called");
     auto blobs = state_blobs(h);
-    size_t need = sizeof(Ctl) + sizeof(long long) + sizeof(int) + sizeof(double) * (1 + h->tstops.size());
-    for (auto& b : blobs) need += b.bytes;
+    const size_t need = ck_size(blobs, h->tstops.size());
     if (!buf) { *size = need; return FI_OK; }
     if (*size < need) return set_err(h, FI_ERR_ARG, "checkpoint buffer too small");
     RET(read_ctl(h));
+    CkHeader hd{};
+    memcpy(hd.magic, CK_MAGIC, sizeof(CK_MAGIC));
+    hd.version = CK_VERSION;
+    hd.form = h->cfg.form;
+    hd.nx = h->nx;
+    hd.ny = h->ny;
+    hd.ctl_bytes = (uint32_t)sizeof(Ctl);
+    hd.nblobs = (uint32_t)blobs.size();
+    hd.nts = h->tstops.size();
+    hd.total = need;
     char* w = (char*)buf;
+    memcpy(w, &hd, sizeof(hd)); w += sizeof(hd);
     memcpy(w, &h->ctl, sizeof(Ctl)); w += sizeof(Ctl);
     memcpy(w, &h->nf_plain, sizeof(long long)); w += sizeof(long long);
     int ls = h->last_call;
     memcpy(w, &ls, sizeof(int)); w += sizeof(int);
-    double nts = (double)h->tstops.size();
-    memcpy(w, &nts, sizeof(double)); w += sizeof(double);
     memcpy(w, h->tstops.data(), h->tstops.size() * sizeof(double)); w += h->tstops.size() * sizeof(double);
     for (auto& b : blobs) {
         CK(cudaMemcpyAsync(w, b.d, b.bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -2232,32 +2364,71 @@ extern "C" int fi_checkpoint(fi_handle* h, void* buf, size_t* size) {
     return FI_OK;
 }
 
+// Every check runs on the caller's bytes before any handle state changes: a rejected
+// checkpoint leaves the handle as it was.
 extern "C" int fi_restore(fi_handle* h, const void* buf, size_t size) {
     if (h) cudaSetDevice(h->cfg.device);
     if (!h || !buf) return FI_ERR_ARG;
     if (!h->initialized) return set_err(h, FI_ERR_STATE, "fi_init must precede fi_restore");
-    const char* r = (const char*)buf;
-    if (size < sizeof(Ctl) + sizeof(long long) + sizeof(int) + sizeof(double))
-        return set_err(h, FI_ERR_ARG, "checkpoint too small");
-    memcpy(&h->ctl, r, sizeof(Ctl)); r += sizeof(Ctl);
-    memcpy(&h->nf_plain, r, sizeof(long long)); r += sizeof(long long);
+    if (size < sizeof(CkHeader)) return set_err(h, FI_ERR_ARG, "checkpoint truncated: %zu bytes", size);
+    CkHeader hd;
+    memcpy(&hd, buf, sizeof(hd));
+    if (memcmp(hd.magic, CK_MAGIC, sizeof(CK_MAGIC)) || hd.version != CK_VERSION)
+        return set_err(h, FI_ERR_ARG, "not a checkpoint of this library version");
+    if (hd.form != h->cfg.form || hd.nx != h->nx || hd.ny != h->ny || hd.ctl_bytes != sizeof(Ctl))
+        return set_err(h, FI_ERR_ARG, "checkpoint of form %d on %d x %d does not match this handle (form %d, %d x %d)",
+                       hd.form, hd.nx, hd.ny, h->cfg.form, h->nx, h->ny);
+    auto blobs = state_blobs(h);
+    if (hd.nblobs != blobs.size()) return set_err(h, FI_ERR_ARG, "checkpoint state layout mismatch");
+    const size_t fixed = ck_size(blobs, 0);
+    if (size < fixed || hd.nts > (size - fixed) / sizeof(double) || hd.nts > (uint64_t)MAX_TSTOPS + 8)
+        return set_err(h, FI_ERR_ARG, "checkpoint truncated or tstop count %llu out of range",
+                       (unsigned long long)hd.nts);
+    const size_t need = ck_size(blobs, (size_t)hd.nts);
+    if (size < need || hd.total != need) return set_err(h, FI_ERR_ARG, "checkpoint size mismatch");
+    const char* r = (const char*)buf + sizeof(hd);
+    Ctl ct;
+    memcpy(&ct, r, sizeof(Ctl)); r += sizeof(Ctl);
+    long long nf_plain;
+    memcpy(&nf_plain, r, sizeof(long long)); r += sizeof(long long);
     int ls;
     memcpy(&ls, r, sizeof(int)); r += sizeof(int);
-    h->last_call = ls;
-    double nts;
-    memcpy(&nts, r, sizeof(double)); r += sizeof(double);
-    h->tstops.assign((const double*)r, (const double*)r + (size_t)nts);
-    r += (size_t)nts * sizeof(double);
-    auto blobs = state_blobs(h);
-    size_t need = (size_t)(r - (const char*)buf);
-    for (auto& b : blobs) need += b.bytes;
-    if (size < need) return set_err(h, FI_ERR_ARG, "checkpoint size mismatch");
+    std::vector<double> ts((size_t)hd.nts);
+    memcpy(ts.data(), r, ts.size() * sizeof(double)); r += ts.size() * sizeof(double);
+    // the step record / replay buffers belong to this handle, not to the checkpoint
+    if (h->cfg.form == FI_FORM_FP32) RET(read_ctl(h));
+    ct.replay_dt = h->ctl.replay_dt;
+    ct.rec_dt = h->ctl.rec_dt;
+    ct.replay_n = h->ctl.replay_n;
+    ct.replay_i = h->ctl.replay_i;
+    ct.rec_cap = h->ctl.rec_cap;
+    ct.rec_n = h->ctl.rec_n;
     for (auto& b : blobs) {
         CK(cudaMemcpyAsync(b.d, r, b.bytes, cudaMemcpyHostToDevice, h->stream));
         r += b.bytes;
     }
+    h->ctl = ct;
+    h->nf_plain = nf_plain;
+    h->last_call = ls;
+    h->tstops.swap(ts);
     RET(write_ctl(h));
     CK(cudaStreamSynchronize(h->stream));
     h->integ_started = true;
     return FI_OK;
+}
+
+namespace fi {
+void tc_set_wait_polls(long long polls);  // fno_gemm.cu
+}
+
+extern "C" int fi_debug_set_wait_limit(int32_t which, int64_t value) {
+    switch (which) {
+        case FI_WAIT_GRID_POLLS: g_grid_polls.store(value < 0 ? -1 : value); return FI_OK;
+        case FI_WAIT_GRID_EXTRA_ARRIVALS:
+            if (value > 1024) return FI_ERR_ARG;
+            g_grid_extra.store(value < 0 ? 0 : value);
+            return FI_OK;
+        case FI_WAIT_TC_POLLS: fi::tc_set_wait_polls(value < 0 ? -1 : value); return FI_OK;
+        default: return FI_ERR_ARG;
+    }
 }

@@ -71,7 +71,11 @@ __host__ __device__ inline int controller_update_pw(Ctl* c, double EEst, double 
         if (q < 1.0 / QMAX) q = 1.0 / QMAX;
     }
     const double ttmp = c->t + c->dt;
-    c->accept_step = EEst <= 1.0;
+    // replay: this attempt took replay_dt[replay_i - 1]; its sign is the decision
+    const bool replay = c->replay_n > 0 && c->replay_i <= c->replay_n;
+    c->accept_step = replay ? (c->replay_dt[c->replay_i - 1] > 0.0) : (EEst <= 1.0);
+    if (c->rec_dt && c->rec_n < c->rec_cap) c->rec_dt[c->rec_n] = c->accept_step ? c->dt : -c->dt;
+    c->rec_n += 1;
     if (c->accept_step) {
         c->naccept += 1;
         c->qold = EEst > QOLDINIT ? EEst : QOLDINIT;
@@ -82,6 +86,11 @@ __host__ __device__ inline int controller_update_pw(Ctl* c, double EEst, double 
         double dp = dtnew < c->dtmax ? dtnew : c->dtmax;
         const double dm = dtmin_at(c->dtmin, c->t);
         c->dtpropose = dp > dm ? dp : dm;
+        if (replay) {
+            // the recorded sequence: the next attempt takes the next recorded dt
+            if (c->replay_i < c->replay_n) c->dtpropose = fabs(c->replay_dt[c->replay_i]);
+            c->replay_i += 1;
+        }
         c->dt = c->dtpropose;  // apply_step!
         c->ibuf ^= 1;
         c->ik ^= 1;
@@ -90,6 +99,10 @@ __host__ __device__ inline int controller_update_pw(Ctl* c, double EEst, double 
         c->nreject += 1;
         const double qq = c->q11 / GAMMA;
         c->dt /= (1.0 / QMIN < qq ? 1.0 / QMIN : qq);
+        if (replay) {
+            if (c->replay_i < c->replay_n) c->dt = fabs(c->replay_dt[c->replay_i]);
+            c->replay_i += 1;
+        }
     }
     return c->accept_step;
 }

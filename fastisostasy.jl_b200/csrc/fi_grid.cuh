@@ -12,10 +12,11 @@
 
 namespace fi {
 
-constexpr long long PERSIST_SPIN_LIMIT = 1LL << 24;  // polls of >= 64 ns each, about 1 s or more
 
 // Returns false (in every thread of the block) when the barrier was abandoned.
-__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, int* s_ok) {
+// polls: the wait bound (PERSIST_SPIN_LIMIT unless a test lowers it).
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, int* s_ok,
+                                             long long polls = PERSIST_SPIN_LIMIT) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned int* vgen = bar + 1;
@@ -29,10 +30,10 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nbl
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
-            long long polls = 0;
+            long long npoll = 0;
             while (*vgen == gen) {
                 if (*vabort) { ok = 0; break; }
-                if (++polls > PERSIST_SPIN_LIMIT) {
+                if (++npoll > polls) {
                     atomicExch(bar + 2, 1u);
                     ok = 0;
                     break;

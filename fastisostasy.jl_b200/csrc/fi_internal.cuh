@@ -56,6 +56,14 @@ struct Ctl {
     double dz_corner[4];
     unsigned int arrive;        // last-block counter of the error-norm reduction
     unsigned int arrive_pad;
+    // Step-sequence replay and record (fi_set_step_replay / fi_record_steps): device
+    // pointers in the FP32 form, host pointers in the plain form (host controller).
+    // Every attempt appends its dt to rec_dt (up to rec_cap), negated when rejected.
+    // While a replay runs, attempt i takes |replay_dt[i]| and is accepted iff
+    // replay_dt[i] > 0.
+    const double* replay_dt;
+    double* rec_dt;
+    long long replay_n, replay_i, rec_cap, rec_n;
 };
 
 // Shared-memory layout of the forward row phase: byte offsets (16-byte aligned) of the

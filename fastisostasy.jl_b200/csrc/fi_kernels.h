@@ -32,6 +32,7 @@ size_t conv_rows_smem(int Mx, int h);
 size_t conv_cols_smem(int My, int B);
 
 // ---- persistent step executor (fi_persist.cu) ----
+constexpr long long PERSIST_SPIN_LIMIT = 1LL << 24;  // grid-barrier polls of >= 64 ns each, about 1 s or more
 struct PersistArgs {
     const Member* mem;
     unsigned int* bar;  // grid barrier: [0] arrivals, [1] generation, [2] abort
@@ -41,6 +42,10 @@ struct PersistArgs {
     int tw_off[4];      // float2 offsets (after the workspace) of the x, y, Mx, My twiddles; -1: global
     int tice_off;       // float2 offset of the ice-time table, -1: read from global memory
     unsigned long long* trace;  // optional phase timeline: [2 * PH_COUNT] sums of ns and counts
+    long long polls;            // grid-barrier wait bound (PERSIST_SPIN_LIMIT by default)
+    unsigned int bar_extra;     // arrivals a barrier expects beyond the grid (0; > 0 only in
+                                // the timeout test, which then sees FI_ERR_TIMEOUT)
+    unsigned int pad_;
 };
 // phases of the persistent executor, as accumulated in PersistArgs::trace
 enum {

@@ -42,6 +42,7 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
     __shared__ int s_ok;
     const int tid = threadIdx.x, bid = blockIdx.x;
     const unsigned int G = gridDim.x;
+    const unsigned int GB = G + a.bar_extra;  // arrivals a grid barrier waits for
 
     // ---- stage the member, the control block, the plans and the ice times ----
     copy_words(&sm, a.mem, sizeof(Member));
@@ -92,15 +93,15 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
             if (sc.gate) {
                 // sparse update: the convolutions read the column anomalies of the last call
                 for (int t = bid; t < a.n_crow; t += G) ph_conv_rows(m, pl[2], smem, t, a.h_conv);
-                if (!(ok = grid_barrier(a.bar, G, &s_ok))) break;
+                if (!(ok = grid_barrier(a.bar, GB, &s_ok, a.polls))) break;
                 trace_mark(trace, &tlast, PH_CONV_ROWS);
                 for (int t = bid; t < a.n_ccol; t += G) ph_conv_cols(m, pl[3], smem, t, a.B_conv);
-                if (!(ok = grid_barrier(a.bar, G, &s_ok))) break;
+                if (!(ok = grid_barrier(a.bar, GB, &s_ok, a.polls))) break;
                 trace_mark(trace, &tlast, PH_CONV_COLS);
                 const int iue = sc.iue;
                 for (int t = bid; t < a.n_crowi; t += G)
                     ph_conv_rows_inv(m, pl[2], smem, t, a.h_conv, iue, m.ctl->ue_corner[iue], m.ctl->dz_corner);
-                if (!(ok = grid_barrier(a.bar, G, &s_ok))) break;
+                if (!(ok = grid_barrier(a.bar, GB, &s_ok, a.polls))) break;
                 trace_mark(trace, &tlast, PH_CONV_ROWS_INV);
                 if (tid < 4) {
                     const volatile double* ue_c = m.ctl->ue_corner[iue];
@@ -142,7 +143,7 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
                     __syncthreads();
                 }
             }
-            if (!(ok = grid_barrier(a.bar, G, &s_ok))) break;
+            if (!(ok = grid_barrier(a.bar, GB, &s_ok, a.polls))) break;
             trace_mark(trace, &tlast, PH_ROWS_FWD2 + 2 * (stage - 2));
             // ---- columns; count the call and evaluate the gate of the next one ----
             for (int tc = bid; tc < a.n_cols; tc += G)
@@ -151,7 +152,7 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
                 sc.nf += 1;
                 if (stage < 4) gate_eval(m, &sc, sc.t + (stage == 2 ? C3 : 1.0) * sc.dt);
             }
-            if (!(ok = grid_barrier(a.bar, G, &s_ok))) break;
+            if (!(ok = grid_barrier(a.bar, GB, &s_ok, a.polls))) break;
             trace_mark(trace, &tlast, PH_COLS2 + 2 * (stage - 2));
         }
         if (!ok) break;
@@ -191,7 +192,7 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
             if (tid == 0)
                 for (int q = 0; q < 4; q++) sc.kcorner[ik ^ 1][q] = s_c4[q];
         }
-        if (!(ok = grid_barrier(a.bar, G, &s_ok))) break;
+        if (!(ok = grid_barrier(a.bar, GB, &s_ok, a.polls))) break;
         trace_mark(trace, &tlast, PH_ROWS_INV4);
         // ---- step controller, replicated: the partials in a fixed order per lane ----
         if (tid < 32) {

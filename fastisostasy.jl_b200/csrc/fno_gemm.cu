@@ -3,7 +3,44 @@
 #include "../../include/fastiso_b200.h"
 #include "fno_gemm.cuh"
 
+#include <atomic>
+#include <mutex>
+
 using namespace fi;
+
+namespace fi {
+
+static std::atomic<long long> g_tc_polls{TC_SPIN_LIMIT};
+long long tc_wait_polls() { return g_tc_polls.load(); }
+void tc_set_wait_polls(long long polls) { g_tc_polls.store(polls < 0 ? TC_SPIN_LIMIT : polls); }
+
+// The status word of fi_fno_gemm: one static device int.  Its address on each device is
+// looked up once (cudaGetSymbolAddress with that device current) and cached.
+static __device__ int g_gemm_err;
+
+namespace {
+constexpr int GEMM_MAX_DEVICES = 64;
+std::mutex g_err_mu;
+int* g_err_ptr[GEMM_MAX_DEVICES] = {};
+
+cudaError_t gemm_err_word(int** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= GEMM_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_err_mu);
+    if (!g_err_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_gemm_err);
+        if (e != cudaSuccess) return e;
+        g_err_ptr[dev] = (int*)p;
+    }
+    *out = g_err_ptr[dev];
+    return cudaSuccess;
+}
+}  // namespace
+
+}  // namespace fi
 
 // C[z] = A[z] * B[z]^T, BF16 inputs, FP32 output; device pointers.  flags bit 0: A is
 // MN-major (element (m, k) at A[k * lda + m]), bit 1: B is MN-major.
@@ -15,8 +52,10 @@ extern "C" int fi_fno_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32
         return FI_ERR_ARG;  // 16-byte vector copies
     if ((amn ? M : K) % 8 || (bmn ? N : K) % 8 || K % 8) return FI_ERR_ARG;
     int* d_err = nullptr;
-    if (cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) return FI_ERR_CUDA;
-    cudaMemset(d_err, 0, sizeof(int));
+    if (gemm_err_word(&d_err) != cudaSuccess) return FI_ERR_CUDA;
+    // stream 0 (legacy) orders the clear, the GEMM and the read-back; calls from several
+    // host threads share the word and are serialised by that stream
+    if (cudaMemsetAsync(d_err, 0, sizeof(int), 0) != cudaSuccess) return FI_ERR_CUDA;
     TcGemmArgs g;
     g.M = M;
     g.N = N;
@@ -35,8 +74,8 @@ extern "C" int fi_fno_gemm(int32_t M, int32_t N, int32_t K, const void* A, int32
                   : N <= 64 ? launch_gemm_tc<64>(g, batch, epi, 0)
                             : launch_gemm_tc<128>(g, batch, epi, 0);
     int herr = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(d_err);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) return FI_ERR_CUDA;
     return herr ? herr : FI_OK;
 }

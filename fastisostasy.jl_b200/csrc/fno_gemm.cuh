@@ -76,9 +76,9 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// bounded wait; false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (long long i = 0; i < TC_SPIN_LIMIT; i++)
+// bounded wait of at most `polls` tests; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long polls = TC_SPIN_LIMIT) {
+    for (long long i = 0; i < polls; i++)
         if (mbar_test(bar, parity)) return true;
     return false;
 }
@@ -152,7 +152,12 @@ struct TcGemmArgs {
     // two-level batch: with zdiv > 1 batch z is (z / zdiv, z % zdiv), else (z, 0)
     int zdiv = 1;
     int* err = nullptr;  // set to FI_ERR_TIMEOUT when a wait gives up
+    long long polls = TC_SPIN_LIMIT;  // bound of each commit wait (tc_wait_polls())
 };
+
+// Poll bound of the commit waits for the next launches: TC_SPIN_LIMIT unless a test
+// lowered it with fi_debug_set_wait_limit (fno_gemm.cu).
+long long tc_wait_polls();
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
@@ -257,12 +262,14 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(TcGemmArgs g, Epi epi) {
         tc_stage<BN>(sa + A_BYTES, g.B, g.B2, z1, z2, n0, g.N, c * TC_BK, g.K, K1, g.A.p);
         cp_async_commit();
     };
+    long long last_commit = -1;  // thread 0: the last job whose MMAs were committed
     if (njobs > 0) stage(0);
     for (long long j = 0; j < njobs; j++) {
         const int s = (int)(j & 1);
         if (j + 1 < njobs) {
             // the other stage buffer was last read by the MMAs of job j - 1
-            if (j >= 1 && tid == 0 && !mbar_wait(&bars[(j - 1) & 1], (uint32_t)(((j - 1) >> 1) & 1))) s_fail = 1;
+            if (j >= 1 && tid == 0 && !mbar_wait(&bars[(j - 1) & 1], (uint32_t)(((j - 1) >> 1) & 1), g.polls))
+                s_fail = 1;
             __syncthreads();
             if (s_fail) break;
             stage(j + 1);
@@ -287,10 +294,11 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(TcGemmArgs g, Epi epi) {
                 tc_mma(tmem, da, db, idesc | (amn << 15) | (bmn << 16), (c > 0 || ks > 0) ? 1u : 0u);
             }
             tc_commit(&bars[s]);
+            last_commit = j;
         }
         if (c == nch - 1) {
             // tile complete: wait for its MMAs, read the accumulator, hand rows to the epilogue
-            if (tid == 0 && !mbar_wait(&bars[s], (uint32_t)((j >> 1) & 1))) s_fail = 1;
+            if (tid == 0 && !mbar_wait(&bars[s], (uint32_t)((j >> 1) & 1), g.polls)) s_fail = 1;
             __syncthreads();
             if (s_fail) break;
             tc_fence_after();
@@ -307,7 +315,13 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(TcGemmArgs g, Epi epi) {
         }
     }
     cp_async_wait<0>();
-    if (s_fail && tid == 0 && g.err) atomicExch(g.err, FI_ERR_TIMEOUT);
+    if (s_fail && tid == 0) {
+        if (g.err) atomicExch(g.err, FI_ERR_TIMEOUT);
+        // before the tensor memory is released, let the MMAs already issued finish
+        // (their commit completes every earlier tcgen05 operation of this thread);
+        // bounded again, with the full limit
+        if (last_commit >= 0) mbar_wait(&bars[last_commit & 1], (uint32_t)((last_commit >> 1) & 1));
+    }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tc_dealloc(tmem, BN < 32 ? 32 : BN);
@@ -351,6 +365,7 @@ inline cudaError_t launch_gemm_tc(const TcGemmArgs& g, int batch, const Epi& epi
     }
     TcGemmArgs a = g;
     a.batch = batch;
+    a.polls = tc_wait_polls();
     const long long ntiles =
         (long long)((g.M + TC_BM - 1) / TC_BM) * ((g.N + BN - 1) / BN) * (long long)batch;
     if (ntiles <= 0) return cudaSuccess;

@@ -545,6 +545,39 @@ class Simulation:
         self._check(self.lib.fi_get_stats(self._handle, C.byref(st)), "fi_get_stats")
         return {k: getattr(st, k) for k, _ in abi.FiStats._fields_}
 
+    # -- no reference counterpart: checkpoints and step-sequence record / replay
+    def checkpoint(self) -> bytes:
+        """fi_checkpoint: the integrator and diagnostic state as bytes."""
+        size = C.c_size_t(0)
+        self._check(self.lib.fi_checkpoint(self._handle, None, C.byref(size)), "fi_checkpoint")
+        buf = C.create_string_buffer(size.value)
+        self._check(self.lib.fi_checkpoint(self._handle, buf, C.byref(size)), "fi_checkpoint")
+        return buf.raw[:size.value]
+
+    def restore(self, blob: bytes):
+        """fi_restore of a checkpoint taken from a handle of the same form and grid."""
+        buf = C.create_string_buffer(bytes(blob), len(blob))
+        self._check(self.lib.fi_restore(self._handle, buf, len(blob)), "fi_restore")
+
+    def record_steps(self, cap: int):
+        """fi_record_steps: store the dt of the next `cap` accepted steps."""
+        self._check(self.lib.fi_record_steps(self._handle, int(cap)), "fi_record_steps")
+
+    def step_record(self) -> np.ndarray:
+        """The recorded accepted step sizes (fi_get_step_record)."""
+        n = C.c_int64(0)
+        self._check(self.lib.fi_get_step_record(self._handle, None, 0, C.byref(n)), "fi_get_step_record")
+        out = np.empty(max(1, n.value))
+        self._check(self.lib.fi_get_step_record(self._handle, abi.dptr(out), n.value, C.byref(n)),
+                    "fi_get_step_record")
+        return out[:n.value].copy()
+
+    def set_step_replay(self, dts):
+        """fi_set_step_replay: the next len(dts) attempts take these step sizes and are accepted."""
+        d = abi.as_f64(dts)
+        self._check(self.lib.fi_set_step_replay(self._handle, d.size, abi.dptr(d) if d.size else None),
+                    "fi_set_step_replay")
+
     @property
     def now(self):
         return _NowView(self)

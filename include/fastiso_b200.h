@@ -215,7 +215,10 @@ int fi_rhs(fi_handle* h, double t, double* u_inout, double* dudt_out);
  * device current); make that first call before any stream capture starts.  All
  * handles on a device share the scratch: calls that overlap in time on one
  * device (from several host threads) race on it and must be serialised by the
- * caller.  The call returns after its device work has finished. */
+ * caller.  The call returns after its device work has finished.  The cached
+ * scratch address belongs to the device's primary context: like every handle, it
+ * does not survive cudaDeviceReset (create new handles after a reset, and do not
+ * call fi_rhs_noalloc again in that process). */
 #define FI_NOALLOC_MAX_CELLS (1024 * 1024)
 int fi_rhs_noalloc(fi_handle* h, double t, double* u_dev, double* dudt_dev);
 
@@ -231,11 +234,32 @@ int fi_run(fi_handle* h, int32_t n_out, const double* t_out, double* out_t,
 int fi_init_integrator(fi_handle* h, int32_t n_tstops, const double* tstops);
 int fi_step(fi_handle* h, double dt);
 
+/* No counterpart in the reference (whose step sequence is OrdinaryDiffEq's own):
+ * record and replay of the accepted step sizes, to separate the arithmetic error of
+ * one compute form from the effect of a different accept/reject sequence.
+ * fi_record_steps(h, cap): from now on the dt of every accepted step is stored (the
+ * first cap of them; cap = 0 stops recording).  fi_get_step_record copies up to cap
+ * stored values into dts and writes into *n how many steps were accepted since
+ * recording started (more than stored when the record overflowed).
+ * fi_set_step_replay(h, n, dts): the next n step attempts take exactly the step
+ * sizes dts[0..n) and are all accepted (no error control); afterwards the adaptive
+ * controller resumes from the last step.  Both need fi_init_integrator; a run that
+ * replays the record of another handle with the same inputs and tstops visits the
+ * same times, so the two solutions can be compared at every output. */
+int fi_record_steps(fi_handle* h, int64_t cap);
+int fi_get_step_record(fi_handle* h, double* dts, int64_t cap, int64_t* n);
+int fi_set_step_replay(fi_handle* h, int64_t n, const double* dts);
+
 /* Counters of the integrator and the RHS. */
 int fi_get_stats(fi_handle* h, fi_stats* st);
 
-/* Checkpoint: the full integrator + diagnostic state.  fi_checkpoint with
- * buf == NULL writes the needed size into *size. */
+/* Checkpoint: the full integrator + diagnostic state, behind a header that names the
+ * library's checkpoint version, the compute form and the grid.  fi_checkpoint with
+ * buf == NULL writes the needed size into *size.  fi_restore checks the header, the
+ * size and the tstop count against the handle before it changes anything: a
+ * checkpoint of another form, grid or version, a truncated buffer or a corrupt count
+ * is rejected with FI_ERR_ARG and leaves the handle as it was.  A recording or replay
+ * installed on the handle (fi_record_steps, fi_set_step_replay) is kept. */
 int fi_checkpoint(fi_handle* h, void* buf, size_t* size);
 int fi_restore(fi_handle* h, const void* buf, size_t size);
 
@@ -324,6 +348,19 @@ void* fi_fno_grads_device(fi_fno* h);
 int fi_fno_set_adam(fi_fno* h, float beta1, float beta2, float eps); /* default 0.9, 0.999, 1e-8 */
 const char* fi_fno_last_error(const fi_fno* h);
 void fi_fno_destroy(fi_fno* h);
+
+/* Diagnostics (no counterpart in the reference): bounds of the library's device
+ * waits, process-wide, for the launches that follow.  FI_WAIT_GRID_POLLS: polls of a
+ * grid-barrier wait in the persistent step kernel (default 2^24, >= 1 s);
+ * FI_WAIT_GRID_EXTRA_ARRIVALS: arrivals a grid barrier expects beyond the launched
+ * grid (default 0; a positive value makes every barrier wait run out, which the
+ * kernel reports as FI_ERR_TIMEOUT); FI_WAIT_TC_POLLS: polls of a tensor-core commit
+ * wait in the surrogate's GEMMs (default 2^26; 0 makes the first wait give up at
+ * once: the kernel then lets its issued MMAs finish, frees its tensor memory and
+ * reports FI_ERR_TIMEOUT).  value < 0 restores the default.  Tests use this to show
+ * that an expired wait returns an error and leaves the context usable. */
+enum { FI_WAIT_GRID_POLLS = 0, FI_WAIT_GRID_EXTRA_ARRIVALS = 1, FI_WAIT_TC_POLLS = 2 };
+int fi_debug_set_wait_limit(int32_t which, int64_t value);
 
 const char* fi_last_error(const fi_handle* h);
 const char* fi_status_string(int32_t status);

@@ -194,6 +194,12 @@ typedef struct {
     const double* tout;
     void (*record)(void* ctx, int k, double t);
     int status;
+    /* step-sequence replay / record (same semantics as the library's
+       fi_set_step_replay / fi_record_steps) */
+    double* replay;
+    int64_t replay_n, replay_i;
+    double* rec;
+    int64_t rec_cap, rec_n;
 } or_integ;
 
 struct or_sim {
@@ -541,7 +547,7 @@ void or_destroy(or_sim* s) {
     fft_plan_free(&s->fx); fft_plan_free(&s->fy); fft_plan_free(&s->fMx); fft_plan_free(&s->fMy);
     or_integ* I = &s->I;
     free(I->u); free(I->uprev); free(I->k1); free(I->k2); free(I->k3); free(I->k4); free(I->tmp);
-    free(I->utilde); free(I->tstops);
+    free(I->utilde); free(I->tstops); free(I->replay); free(I->rec);
     free(s);
 }
 
@@ -987,6 +993,14 @@ static int integ_attempt(or_integ* I) {
             const double q = I->q11 / CTRL_GAMMA;
             I->dt /= (1.0 / CTRL_QMIN < q ? 1.0 / CTRL_QMIN : q);
         }
+        /* a replayed sequence: this attempt takes the next recorded dt */
+        if (I->replay_n > 0 && I->replay_i <= I->replay_n) {
+            if (I->replay_i < I->replay_n) {
+                I->dt = fabs(I->replay[I->replay_i]);
+                I->dtpropose = I->dt;
+            }
+            I->replay_i++;
+        }
     }
     I->iter += 1;
     /* fix_dt_at_bounds!, modify_dt_for_tstops! */
@@ -1037,7 +1051,11 @@ static int integ_attempt(or_integ* I) {
         if (q > 1.0 / CTRL_QMIN) q = 1.0 / CTRL_QMIN;
         if (q < 1.0 / CTRL_QMAX) q = 1.0 / CTRL_QMAX;
     }
-    I->accept_step = I->EEst <= 1.0;
+    /* replay: this attempt took replay[replay_i - 1]; its sign is the decision */
+    const int replay = I->replay_n > 0 && I->replay_i <= I->replay_n;
+    I->accept_step = replay ? (I->replay[I->replay_i - 1] > 0.0) : (I->EEst <= 1.0);
+    if (I->rec && I->rec_n < I->rec_cap) I->rec[I->rec_n] = I->accept_step ? I->dt : -I->dt;
+    I->rec_n++;
     if (I->accept_step) {
         I->naccept++;
         /* step_accept_controller! */
@@ -1164,6 +1182,41 @@ int or_step(or_sim* s, double dt) {
     if (!s || !(dt > 0)) return FI_ERR_ARG;
     if (!s->I.initialized) return set_err(s, FI_ERR_STATE, "or_init_integrator not called");
     return integ_step_to(&s->I, dt);
+}
+
+int or_record_steps(or_sim* s, int64_t cap) {
+    if (!s || cap < 0) return FI_ERR_ARG;
+    if (!s->I.initialized) return set_err(s, FI_ERR_STATE, "or_init_integrator not called");
+    free(s->I.rec);
+    s->I.rec = cap > 0 ? dalloc((size_t)cap) : NULL;
+    s->I.rec_cap = cap;
+    s->I.rec_n = 0;
+    return FI_OK;
+}
+
+int or_get_step_record(or_sim* s, double* dts, int64_t cap, int64_t* n) {
+    if (!s || !n || cap < 0 || (cap > 0 && !dts)) return FI_ERR_ARG;
+    int64_t k = s->I.rec_n < s->I.rec_cap ? s->I.rec_n : s->I.rec_cap;
+    if (k > cap) k = cap;
+    if (k > 0) memcpy(dts, s->I.rec, (size_t)k * sizeof(double));
+    *n = s->I.rec_n;
+    return FI_OK;
+}
+
+int or_set_step_replay(or_sim* s, int64_t n, const double* dts) {
+    if (!s || n < 0 || (n > 0 && !dts)) return FI_ERR_ARG;
+    if (!s->I.initialized) return set_err(s, FI_ERR_STATE, "or_init_integrator not called");
+    free(s->I.replay);
+    s->I.replay = NULL;
+    if (n > 0) {
+        s->I.replay = dalloc((size_t)n);
+        memcpy(s->I.replay, dts, (size_t)n * sizeof(double));
+        s->I.dt = fabs(dts[0]);
+        s->I.dtpropose = fabs(dts[0]);
+    }
+    s->I.replay_n = n;
+    s->I.replay_i = n > 0 ? 1 : 0;
+    return FI_OK;
 }
 
 int or_get_stats(or_sim* s, fi_stats* st) {

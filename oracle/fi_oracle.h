@@ -30,6 +30,9 @@ int or_run(or_sim* s, int32_t n_out, const double* t_out, double* out_t,
            double* out_u, double* out_ue, double* out_dudt, double* out_dz_ss);
 int or_init_integrator(or_sim* s, int32_t n_tstops, const double* tstops);
 int or_step(or_sim* s, double dt);
+int or_record_steps(or_sim* s, int64_t cap);
+int or_get_step_record(or_sim* s, double* dts, int64_t cap, int64_t* n);
+int or_set_step_replay(or_sim* s, int64_t n, const double* dts);
 int or_get_stats(or_sim* s, fi_stats* st);
 const char* or_last_error(const or_sim* s);
 void or_destroy(or_sim* s);

@@ -45,6 +45,9 @@ def lib():
         "or_init_integrator": (C.c_int, [C.c_void_p, C.c_int32, dp]),
         "or_step": (C.c_int, [C.c_void_p, C.c_double]),
         "or_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FiStats)]),
+        "or_record_steps": (C.c_int, [C.c_void_p, C.c_int64]),
+        "or_get_step_record": (C.c_int, [C.c_void_p, dp, C.c_int64, C.POINTER(C.c_int64)]),
+        "or_set_step_replay": (C.c_int, [C.c_void_p, C.c_int64, dp]),
         "or_last_error": (C.c_char_p, [C.c_void_p]),
         "or_destroy": (None, [C.c_void_p]),
         "or_set_threads": (None, [C.c_int32]),
@@ -140,6 +143,21 @@ class OracleSim:
 
     def step(self, dt):
         self._check(lib().or_step(self.h, float(dt)), "step")
+
+    def record_steps(self, cap):
+        self._check(lib().or_record_steps(self.h, int(cap)), "record_steps")
+
+    def step_record(self, cap=None):
+        n = C.c_int64()
+        self._check(lib().or_get_step_record(self.h, None, 0, C.byref(n)), "get_step_record")
+        k = n.value if cap is None else min(n.value, cap)
+        out = np.empty(max(k, 1))
+        self._check(lib().or_get_step_record(self.h, _p(out), k, C.byref(n)), "get_step_record")
+        return out[:min(k, n.value)]
+
+    def set_step_replay(self, dts):
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        self._check(lib().or_set_step_replay(self.h, dts.size, _p(dts) if dts.size else None), "set_step_replay")
 
     def stats(self):
         from fastiso_b200.abi import FiStats

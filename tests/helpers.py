@@ -62,3 +62,41 @@ def golden_u(sim, seed=12):
 GOLDEN_RHS_TIMES = (0.5, 12.5)
 GOLDEN_RUN_TIMES = (300.0, 600.0, 1000.0)
 GOLDEN_RUN_T_END = 1000.0
+
+
+def lib_outputs(sim, t_outs, fields=("u", "dudt", "dz_ss"), record=0, replay=None):
+    """Integrate a library Simulation with init_integrator (output times as tstops) and
+    step! to each output time; returns ({field: [flat x-fastest arrays]}, record).
+    record > 0 stores the attempt sequence (fi_record_steps); replay installs one.
+    The output times are the run's tstops with the output callback (nout.t), as the
+    oracle's init_integrator(t_outs) has them."""
+    sim.nout.t = [float(t) for t in t_outs]
+    integ = F.init_integrator(sim)
+    if record:
+        sim.record_steps(record)
+    if replay is not None:
+        sim.set_step_replay(replay)
+    out = {f: [] for f in fields}
+    for t in t_outs:
+        F.step(integ, t - integ.t, True)
+        for f in fields:
+            out[f].append(F_(sim.get_field(f)))
+    return out, (sim.step_record() if record else None)
+
+
+ORACLE_FIELD_IDS = {"u": 8, "dudt": 10, "dz_ss": 11, "ue": 9}
+
+
+def oracle_outputs(ref, t_outs, fields=("u", "dudt", "dz_ss"), record=0, replay=None):
+    """The same for the oracle (already initialised with ref.init())."""
+    ref.init_integrator(np.asarray(t_outs, dtype=np.float64))
+    if record:
+        ref.record_steps(record)
+    if replay is not None:
+        ref.set_step_replay(replay)
+    out = {f: [] for f in fields}
+    for t in t_outs:
+        ref.step(t - ref.stats()["t"])
+        for f in fields:
+            out[f].append(ref.get_field(ORACLE_FIELD_IDS[f]))
+    return out, (ref.step_record() if record else None)

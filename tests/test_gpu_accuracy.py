@@ -1,0 +1,104 @@
+"""Accuracy of the FP32 form against Float64, with the arithmetic error separated from
+the step sequence.
+
+The reference's adaptive BS3 run (src/simulation.jl:236-262) is sensitive to its own
+accept/reject sequence: the sparse elastic and sea-surface update fires at the stage
+time of whichever attempt crosses the next 10-yr mark, rejected attempts included
+(src/simulation.jl:355-381), so two correct runs whose controllers reject differently
+differ by the integrator's own error (about 4e-4 in u at reltol = 1f-5).  Replaying one
+run's recorded attempt sequence (fi_record_steps / fi_set_step_replay: every dt, each
+with its accept decision) makes another run visit exactly the same stage times, so
+their difference is the arithmetic error alone.
+
+The gate of the FP32 form is rel-L2 <= 1e-4 on u, dudt and dz_ss against Float64 at
+every output time, on the N = 350 glacial-cycle workload (6000 km, seeded random
+viscosity, lithosphere and ice fields, elastic, viscous and sea-surface convolutions).
+"""
+import numpy as np
+import pytest
+
+import fastiso_b200 as F
+import fastiso_b200.workloads as W
+from helpers import lib_outputs, oracle_for, oracle_outputs, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u", "dudt", "dz_ss")
+GATE = 1e-4          # FP32 form vs Float64, same attempt sequence
+FP64_RUN_TOL = 1e-9  # plain FP64 GPU form vs the Float64 oracle, same attempt sequence
+
+
+def _errors(a, b):
+    return {f: [rel_l2(x, y) for x, y in zip(a[f], b[f])] for f in FIELDS}
+
+
+def test_replay_reproduces_the_recorded_run():
+    """The plain FP64 form replaying its own record is bitwise the recorded run, and
+    the oracle replaying the GPU's record agrees with it to FP64 round-off."""
+    t_outs = [50.0, 120.0, 300.0]
+    a = W.config2(form="fp64", N=48, t_end=300.0, out_every=300.0, n_snap=2)
+    out_a, rec = lib_outputs(a, t_outs, record=1 << 20)
+    a.close()
+    assert (rec < 0).any(), "the case should reject some attempts"
+    b = W.config2(form="fp64", N=48, t_end=300.0, out_every=300.0, n_snap=2)
+    out_b, rec_b = lib_outputs(b, t_outs, record=1 << 20, replay=rec)
+    b.close()
+    np.testing.assert_array_equal(rec_b, rec)
+    for f in FIELDS:
+        for x, y in zip(out_a[f], out_b[f]):
+            np.testing.assert_array_equal(x, y)
+    sim = W.config2(form="fp64", N=48, t_end=300.0, out_every=300.0, n_snap=2)
+    ref = oracle_for(sim)
+    ref.init()
+    out_r, _ = oracle_outputs(ref, t_outs, replay=rec)
+    ref.close()
+    sim.close()
+    for f, errs in _errors(out_a, out_r).items():
+        assert max(errs) < FP64_RUN_TOL, (f, errs)
+
+
+def test_fp32_replay_small_against_oracle():
+    """Small case, every field: the FP32 form replaying the oracle's own record."""
+    t_outs = [100.0, 250.0, 500.0]
+    sim = W.config2(form="fp32", N=64, t_end=500.0, out_every=500.0, n_snap=2)
+    ref = oracle_for(sim)
+    ref.init()
+    out_r, rec = oracle_outputs(ref, t_outs, record=1 << 20)
+    ref.close()
+    out_g, _ = lib_outputs(sim, t_outs, replay=rec)
+    sim.close()
+    for f, errs in _errors(out_g, out_r).items():
+        assert max(errs) < GATE, (f, errs)
+
+
+def test_accuracy_gate_config2_n350():
+    """N = 350 glacial cycle, first 1.5 kyr, outputs every 100 yr: the plain FP64 GPU
+    form records its adaptive run; the FP32 form replays it (gate 1e-4 on u, dudt and
+    dz_ss at every output); the Float64 oracle replays the first 100 yr and pins both."""
+    t_outs = [float(t) for t in np.arange(100.0, 1501.0, 100.0)]
+    p = W.config2(form="fp64", N=350)
+    p.cfg.max_steps = 50_000_000
+    out64, rec = lib_outputs(p, t_outs, record=1 << 22)
+    p.close()
+    assert rec.size < (1 << 22)
+    s = W.config2(form="fp32", N=350)
+    s.cfg.max_steps = 50_000_000
+    out32, _ = lib_outputs(s, t_outs, replay=rec)
+    s.close()
+    errs = _errors(out32, out64)
+    print({f: f"max {max(e):.2e}" for f, e in errs.items()})
+    for f, e in errs.items():
+        assert max(e) <= GATE, (f, e)
+    # the oracle on the first output interval (its attempts are a prefix of the record)
+    sim = W.config2(form="fp64", N=350)
+    ref = oracle_for(sim)
+    ref.init()
+    out_r, _ = oracle_outputs(ref, t_outs[:1], replay=rec)
+    ref.close()
+    sim.close()
+    for f in FIELDS:
+        e64 = rel_l2(out64[f][0], out_r[f][0])
+        e32 = rel_l2(out32[f][0], out_r[f][0])
+        print(f, "fp64 vs oracle", e64, "fp32 vs oracle", e32)
+        assert e64 < FP64_RUN_TOL, (f, e64)
+        assert e32 <= GATE, (f, e32)

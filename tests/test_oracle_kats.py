@@ -126,3 +126,36 @@ def test_analytic_disc_load():
         # the corner BC fixes the far field at 0 while the half-space solution does not vanish there
         err = rel_l2(num - num[-1], ana - ana[-1])
         assert err < 0.02, (t, err)
+
+
+def test_oracle_replay_reproduces_its_run():
+    """The attempt record (accepted dt > 0, rejected dt < 0) replayed on a fresh oracle
+    visits the same stage times, rejected attempts and sparse updates included, and
+    reproduces the run bit for bit (the basis of the FP32-vs-Float64 replay tests)."""
+    import fastiso_b200.workloads as W
+
+    t_outs = np.array([100.0, 300.0])
+
+    def fresh():
+        sim = W.config2(form="fp64", N=32, t_end=300.0, out_every=300.0, n_snap=2)
+        r = O.oracle_for(sim)
+        r.init()
+        r.init_integrator(t_outs)
+        return r
+
+    a = fresh()
+    a.record_steps(1 << 16)
+    ua = []
+    for t in t_outs:
+        a.step(t - a.stats()["t"])
+        ua.append(a.get_field(8))
+    rec = a.step_record()
+    st_a = a.stats()
+    assert (rec < 0).sum() == st_a["nreject"] and (rec > 0).sum() == st_a["naccept"]
+    b = fresh()
+    b.set_step_replay(rec)
+    for t, u in zip(t_outs, ua):
+        b.step(t - b.stats()["t"])
+        np.testing.assert_array_equal(b.get_field(8), u)
+    st_b = b.stats()
+    assert (st_b["naccept"], st_b["nreject"], st_b["nsparse"]) == (st_a["naccept"], st_a["nreject"], st_a["nsparse"])

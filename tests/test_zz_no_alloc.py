@@ -68,3 +68,29 @@ def test_rhs_noalloc_rejects_oversized_grid_and_fp64_form():
     s64.init_problem()
     buf = torch.zeros(16 * 16, dtype=torch.float64, device="cuda:0")
     assert _noalloc(s64, 0.0, buf, buf) == abi.FI_ERR_ARG
+
+
+def test_rhs_noalloc_leaves_device_memory_unchanged():
+    """After a first call on the device (which looks up the scratch address), 100 more
+    calls change neither the device's free memory (cudaMemGetInfo) nor torch's
+    reserved pool: the entry point allocates nothing per call."""
+    torch = pytest.importorskip("torch")
+    nx, ny = 48, 40
+    b = _sim(nx, ny)
+    b.init_problem()
+    rng = np.random.default_rng(5)
+    u = -50 * np.exp(-b.domain.R**2 / (2 * (0.3 * b.domain.Wx) ** 2)) + 0.5 * rng.standard_normal((nx, ny))
+    u_dev = torch.from_numpy(F_(u)).to("cuda:0")
+    dudt_dev = torch.empty_like(u_dev)
+    assert _noalloc(b, 0.5, u_dev, dudt_dev) == abi.FI_OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    reserved0 = torch.cuda.memory_reserved(0)
+    for k in range(100):
+        assert _noalloc(b, 0.5 + 0.25 * k, u_dev, dudt_dev) == abi.FI_OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
+    assert torch.cuda.memory_reserved(0) == reserved0
+    assert torch.isfinite(dudt_dev).all()
+    b.close()

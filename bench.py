@@ -375,55 +375,145 @@ def fno_bench(dev, steps, warmup, S=128, B=32):
             "forward_tflops": f * B / (fwd_ms / 1e3) / 1e12}
 
 
-def cpu_oracle_sample(seconds_target=12.0, seg=5.0):
-    """The FP64 oracle on the host cores: config-2 segments of `seg` yr until about
-    `seconds_target` of CPU work; returns (kyr/s, cores, years)."""
+FP64_WINDOW_MAX_KYR = 5  # plain FP64 form and replay accuracy: the first segments of the timed window
+
+
+def fp64_window(dev, warm_kyr, win_kyr):
+    """The plain FP64 form on the headline workload: from t = 0, 1-kyr segments through
+    the warm-up and then `win_kyr` segments of the timed window (the same segments as
+    the FP32 headline).  Records every attempt (fi_record_steps) for the FP32 replay,
+    times each window segment with CUDA events, keeps u, dudt and dz_ss at each window
+    segment end and the state at the window start (for the CPU oracle's resume)."""
+    psim = W.config2(form="fp64", N=N350)
+    psim.cfg.device = dev
+    psim.cfg.max_steps = 50_000_000
+    integ = F.init_integrator(psim)
+    psim.record_steps(1 << 23)
+    seg_ms, fields, start = [], [], None
+    for k in range(warm_kyr + win_kyr):
+        if k == warm_kyr:
+            st = psim.stats()
+            start = {"t": st["t"], "nsparse": st["nsparse"],
+                     "u": psim.get_field("u"), "ue": psim.get_field("ue"), "dz_ss": psim.get_field("dz_ss")}
+            a0 = st["naccept"] + st["nreject"]
+        F.step(integ, SEG_YR, True)
+        if k >= warm_kyr:
+            seg_ms.append(psim.stats()["last_gpu_ms"])
+            fields.append({f: psim.get_field(f) for f in ("u", "dudt", "dz_ss")})
+    st = psim.stats()
+    rec = psim.step_record()
+    psim.close()
+    return {"seg_ms": seg_ms, "fields": fields, "record": rec, "start": start,
+            "attempts": st["naccept"] + st["nreject"] - a0}
+
+
+def fp32_replay_errors(dev, warm_kyr, ref):
+    """The FP32 form replaying the plain FP64 form's attempt sequence from t = 0: the
+    same stage times, sparse updates and accept decisions, so the difference at each
+    window segment end is the FP32 arithmetic error alone."""
+    sim = W.config2(form="fp32", N=N350)
+    sim.cfg.device = dev
+    sim.cfg.max_steps = 50_000_000
+    integ = F.init_integrator(sim)
+    sim.set_step_replay(ref["record"])
+    errs = {f: [] for f in ("u", "dudt", "dz_ss")}
+    for k in range(warm_kyr + len(ref["fields"])):
+        F.step(integ, SEG_YR, True)
+        if k >= warm_kyr:
+            for f in errs:
+                errs[f].append(rel_l2(sim.get_field(f), ref["fields"][k - warm_kyr][f]))
+    sim.close()
+    return errs
+
+
+def rel_l2(a, b):
+    a, b = np.ravel(a), np.ravel(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def oracle_resumed(start, threads, seconds_target, seg=5.0, max_segs=None):
+    """The FP64 oracle (the reference's CPU semantics) resumed at the window start from
+    the plain FP64 form's state, stepping `seg`-yr segments until about
+    `seconds_target` s of CPU work (or max_segs segments); returns (kyr/s, years)."""
     from oracle import oracle as O
 
-    cores = os.cpu_count() or 1
-    O.set_threads(cores)
+    O.set_threads(threads)
     sim = W.config2(form="fp64", N=N350)
     ref = O.oracle_for(sim)
     ref.init()
-    ref.init_integrator([])
-    yrs, t_used = 0.0, 0.0
-    while t_used < seconds_target:
+    F_ = lambda a: np.asarray(a, dtype=np.float64).ravel(order="F")  # noqa: E731
+    ref.resume(start["t"], start["nsparse"], F_(start["u"]), F_(start["ue"]), F_(start["dz_ss"]))
+    yrs, used, n = 0.0, 0.0, 0
+    while used < seconds_target and (max_segs is None or n < max_segs):
         t0 = time.perf_counter()
         ref.step(seg)
-        t_used += time.perf_counter() - t0
+        used += time.perf_counter() - t0
         yrs += seg
-    return yrs / 1e3 / t_used, cores, yrs
+        n += 1
+    ref.close()
+    return yrs / 1e3 / used, yrs
+
+
+def config_block(warm_kyr, world):
+    """The workload description shared by both arms (the reference arm times the same
+    window of the same run)."""
+    return {"workload": "config2 glacial cycle N=350 over 6000 km, 121 ice snapshots, "
+                        "elastic+viscous+sea-surface, BS3 reltol=Float64(1f-5)",
+            "window_start_kyr": warm_kyr,
+            "parallelism": "replicas" if world > 1 else "single"}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's CPU semantics (the FP64 oracle, OpenMP over the
-    host cores), same metric and config; rank 0 only."""
+    """--impl reference: the reference's CPU semantics (the FP64 oracle port, OpenMP over
+    all host cores) on the same window of the same run as the GPU arm: the run is
+    brought to the window start (t = warmup kyr) by the plain FP64 GPU form (outside
+    the timed region), the oracle resumes from that state, and each step is a bounded
+    5-yr sample of the window; rank 0 only."""
     if rank != 0:
         return
     from oracle import oracle as O
 
+    warm = args.warmup
     cores = os.cpu_count() or 1
     O.set_threads(cores)
     seg = 5.0
     sim = W.config2(form="fp64", N=N350)
     ref = O.oracle_for(sim)
     ref.init()
-    ref.init_integrator([])
+    if warm > 0:
+        import torch
+
+        dev = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(dev)
+        p = W.config2(form="fp64", N=N350)
+        p.cfg.device = dev
+        p.cfg.max_steps = 50_000_000
+        integ = F.init_integrator(p)
+        for _ in range(warm):
+            F.step(integ, SEG_YR, True)
+        st = p.stats()
+        F_ = lambda a: np.asarray(a, dtype=np.float64).ravel(order="F")  # noqa: E731
+        ref.resume(st["t"], st["nsparse"], F_(p.get_field("u")), F_(p.get_field("ue")), F_(p.get_field("dz_ss")))
+        p.close()
+    else:
+        ref.init_integrator([])
+    t_start = ref.stats()["t"]
     for _ in range(args.warmup):
         ref.step(seg)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         ref.step(seg)
     el = time.perf_counter() - t0
+    ref.close()
     v = args.steps * seg / 1e3 / el
+    sample = (f"{args.steps} x {seg:g} yr of config2 N=350 from t = {t_start / 1e3:g} kyr + {args.warmup} x "
+              f"{seg:g} yr (the oracle resumed from the plain FP64 GPU form's state at the window start)")
     line = {"metric": METRIC, "value": v, "unit": "kyr/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fields)",
             "impl": "reference",
-            "config": {"workload": "config2 glacial cycle N=350, 6000 km, elastic+viscous+sea-surface",
-                       "step": f"{seg} yr of simulated time per step (bounded CPU sample)"},
-            "cpu_baseline": {"value": v, "unit": "kyr/s", "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} x {seg} yr of config2 after {args.warmup} x {seg} yr warm-up"},
+            "config": config_block(warm, world),
+            "cpu_baseline": {"value": v, "unit": "kyr/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "kyr/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -431,12 +521,13 @@ def run_reference(args, rank, world):
 def run_gpu(args, rank, world, dev):
     import torch
 
+    warm = args.warmup
     # ---- headline: fused FP32 form, inputs resident ------------------------------
     sim = W.config2(form="fp32", N=N350)
     sim.cfg.device = dev
     sim.cfg.max_steps = 20_000_000
     integ = F.init_integrator(sim)
-    for _ in range(args.warmup):
+    for _ in range(warm):
         F.step(integ, SEG_YR, True)
     c0 = counters(sim)
     step_ms = []
@@ -452,6 +543,7 @@ def run_gpu(args, rank, world, dev):
         if world > 1:
             torch.distributed.barrier()
     c1 = counters(sim)
+    u_end = sim.get_field("u")
     phases = phase_timeline(sim, integ) if rank == 0 else None
     sim.close()
     ens = ensemble_bench(dev, rank, world)
@@ -466,79 +558,90 @@ def run_gpu(args, rank, world, dev):
     launches = launches_between(c0, c1, c1["executor"])
     if rank != 0:
         return
-    # ---- e2e: coupling API with host buffers -------------------------------------
-    e2e_sim = W.config2(form="fp32", N=N350)
-    dom = e2e_sim.domain
-    _, _, _, H_field = W.config2_fields(N350, 3e6)
-    bcs = F.BoundaryConditions(dom, ice_thickness=F.ExternallyUpdatedIceThickness())
-    esim = F.Simulation(dom, bcs, e2e_sim.sealevel, e2e_sim.solidearth, (0.0, 120e3), form="fp32", device=dev,
-                        max_steps=20_000_000)
-    e2e_sim.close()
+    assert np.isfinite(u_end).all()
+    # ---- e2e: the public API with host buffers, the same time-interpolated forcing ----
+    # per step: the state u uploaded from pinned host memory (integrator.u .= u, which
+    # makes the next step re-evaluate its FSAL derivative), step!(1 kyr), u read back
+    # into pinned host memory
+    esim = W.config2(form="fp32", N=N350)
+    esim.cfg.device = dev
+    esim.cfg.max_steps = 20_000_000
     einteg = F.init_integrator(esim)
-    H_host = np.ascontiguousarray(H_field)
-    tt = 0.0
-    for _ in range(args.warmup):
-        esim.set_field("H_ice", H_host * W.sawtooth(tt + SEG_YR / 2))
-        F.step(einteg, SEG_YR, True)
-        tt += SEG_YR
-    t0 = time.perf_counter()
+    n = N350 * N350
+    u_pin = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    u_np = u_pin.numpy()
+    lib, hnd = esim.lib, esim._handle
+    from fastiso_b200 import abi
+
+    def e2e_step():
+        esim._check(lib.fi_set_field(hnd, abi.FIELDS["u"], abi.dptr(u_np), n), "set u")
+        esim._check(lib.fi_step(hnd, SEG_YR), "fi_step")
+        esim._check(lib.fi_get_field(hnd, abi.FIELDS["u"], abi.dptr(u_np), n), "get u")
+
+    esim._check(lib.fi_get_field(hnd, abi.FIELDS["u"], abi.dptr(u_np), n), "get u")
+    for _ in range(warm):
+        e2e_step()
+    e2e_el = 0.0
     for _ in range(args.steps):
-        esim.set_field("H_ice", H_host * W.sawtooth(tt + SEG_YR / 2))
-        F.step(einteg, SEG_YR, True)
-        u_host = esim.get_field("u")
-        tt += SEG_YR
-    e2e_el = time.perf_counter() - t0
+        l2_flush(dev)
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_el += time.perf_counter() - t0
     e2e_val = kyr / e2e_el
-    assert np.isfinite(u_host).all()
+    assert np.isfinite(u_np).all()
     esim.close()
-    # ---- plain FP64 form on a short window of the same workload ------------------
-    psim = W.config2(form="fp64", N=N350)
-    psim.cfg.device = dev
-    psim.cfg.max_steps = 20_000_000
-    pinteg = F.init_integrator(psim)
-    F.step(pinteg, 20.0, True)
-    p0 = psim.stats()
-    F.step(pinteg, 20.0, True)
-    p1 = psim.stats()
-    plain_kyr_s = 0.020 / (p1["last_gpu_ms"] / 1e3)
-    plain_ms_per_bs3 = p1["last_gpu_ms"] / max(1, (p1["naccept"] + p1["nreject"]) - (p0["naccept"] + p0["nreject"]))
-    psim.close()
+    # ---- plain FP64 form on the same window; FP32 replay of its attempt sequence ----
+    nwin = min(args.steps, FP64_WINDOW_MAX_KYR)
+    p64 = fp64_window(dev, warm, nwin)
+    plain_kyr_s = nwin / (sum(p64["seg_ms"]) / 1e3)
+    fp32_same = nwin / (sum(step_ms[:nwin]) / 1e3)
+    replay = fp32_replay_errors(dev, warm, p64)
+    acc = {f"relL2_{f}_vs_fp64": max(e) for f, e in replay.items()}
     # ---- roofline of the dominant kernel ----------------------------------------
     seg = max(1, c1["segments"] - c0["segments"])
     roof = roofline(dev, 1e3 * t_total / max(1, attempts), attempts / seg, c1["executor"], c1["grid"])
     # ---- the surrogate network and the N = 1024 case (outside the timed region) ----
     surrogate = fno_bench(dev, 20, max(3, args.warmup))
     config5 = config5_bench(dev)
-    # ---- CPU baseline (oracle) ---------------------------------------------------
-    cpu_v, cores, yrs = cpu_oracle_sample()
+    # ---- CPU baseline: the oracle resumed at the window start --------------------
+    cores = os.cpu_count() or 1
+    cpu_all, yrs_all = oracle_resumed(p64["start"], cores, 12.0)
+    cpu_one, yrs_one = oracle_resumed(p64["start"], 1, 8.0, seg=1.0)
+    win = f"t = {warm}..{warm + nwin} kyr"
     line = {
         "metric": METRIC, "value": value, "unit": "kyr/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 state)",
         "data": "synthetic (seeded Gaussian random fields)",
-        "config": {"workload": "config2 glacial cycle N=350 over 6000 km, 121 ice snapshots, "
-                               "elastic+viscous+sea-surface, BS3 reltol=Float64(1f-5)",
-                   "step": f"{SEG_YR:g} yr of simulated time (consecutive segments)",
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "256 MiB written between timed steps; one member's working set (~15 MB) is "
-                         "L2-resident within a step"},
+        "config": config_block(warm, world),
+        "step": f"{SEG_YR:g} yr of simulated time (consecutive segments from t = {warm} kyr)",
+        "l2": "256 MiB written between timed steps; one member's working set (~15 MB) is L2-resident within a step",
         "bs3_steps_per_bench_step": attempts / args.steps,
         "us_per_bs3_step": 1e3 * t_total / max(1, attempts),
         "rhs_evals_per_s": (c1["nf"] - c0["nf"]) / (t_total / 1e3),
-        "plain_fp64": {"value": plain_kyr_s, "unit": "kyr/s", "ms_per_bs3_step": plain_ms_per_bs3,
-                       "sample": "20 yr after 20 yr warm-up"},
-        "speedup_vs_plain_fp64": value / world / plain_kyr_s,
+        "accuracy": dict(acc, window=win, method="FP32 form replaying the plain FP64 form's recorded attempt "
+                                               "sequence (dt and accept decision of every attempt) from t = 0; "
+                                               "rel-L2 at every 1-kyr segment end, max over the window",
+                         per_segment={f: [float(x) for x in e] for f, e in replay.items()}),
+        **acc,
+        "plain_fp64": {"value": plain_kyr_s, "unit": "kyr/s", "window": win,
+                       "ms_per_bs3_step": sum(p64["seg_ms"]) / max(1, p64["attempts"]),
+                       "fp32_same_window": fp32_same},
+        "speedup_vs_plain_fp64": fp32_same / plain_kyr_s,
         "ensemble": ens,
         "surrogate": surrogate,
         "config5": config5,
-        "e2e": {"value": e2e_val, "unit": "kyr/s", "h2d_bytes_per_step": 8 * N350 * N350,
-                "d2h_bytes_per_step": 8 * N350 * N350,
-                "path": "init_integrator + per step: set H_ice (host) -> step!(1 kyr) -> read u (host)"},
+        "e2e": {"value": e2e_val, "unit": "kyr/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                "path": "per step: fi_set_field(u) from pinned host memory -> fi_step(1 kyr, the resident "
+                        "time-interpolated ice history) -> fi_get_field(u) into pinned host memory; wall clock"},
         "gpu_launches": int(launches),
         "phases": phases,
         "roofline": roof,
-        "cpu_baseline": {"value": cpu_v, "unit": "kyr/s", "cores": cores, "kind": "port",
-                         "sample": f"FP64 oracle (C, OpenMP), config2 N=350, {yrs:g} yr from t=0"},
+        "cpu_baseline": {"value": cpu_all, "unit": "kyr/s", "cores": cores, "kind": "port",
+                         "sample": f"FP64 oracle (C, OpenMP) resumed at t = {warm} kyr from the plain FP64 form's "
+                                   f"state, {yrs_all:g} yr",
+                         "single_thread": {"value": cpu_one, "unit": "kyr/s", "cores": 1,
+                                           "sample": f"the same, 1 thread, {yrs_one:g} yr"}},
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)

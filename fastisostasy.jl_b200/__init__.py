@@ -15,3 +15,8 @@ from .model import (  # noqa: F401
     SolverOptions, TimeInterpolatedIceThickness, UnsupportedError, get_greenintegrand_coeffs, get_rigidity,
     init_integrator, nextfastfft, run, samesize_conv_indices, step, update_diagnostics,
 )
+from .model import (  # noqa: F401
+    ConstantOceanSurfaceBSL, ExternalBSLUpdate, GoelzerAdjustmentContribution, GoelzerDensityContribution,
+    GoelzerVolumeContribution, ImposedBSL, InteractiveSealevelLoad, InternalBSLUpdate, NoAdjustmentContribution,
+    NoDensityContribution, NoVolumeContribution, PiecewiseConstantBSL, ReferenceBSL,
+)

@@ -38,6 +38,18 @@ FI_COLUMN_INCOMPRESSIBLE = 0
 FI_COLUMN_COMPRESSIBLE = 1
 FI_ICE_TIME_INTERPOLATED = 0
 FI_ICE_EXTERNAL = 1
+FI_SEALEVEL_LOAD_NONE = 0
+FI_SEALEVEL_LOAD_INTERACTIVE = 1
+FI_BSL_CONSTANT = 0
+FI_BSL_CONSTANT_OCEAN_SURFACE = 1
+FI_BSL_PIECEWISE_CONSTANT = 2
+FI_BSL_IMPOSED = 3
+FI_BSL_UPDATE_INTERNAL = 0
+FI_BSL_UPDATE_EXTERNAL = 1
+FI_CONTRIB_NONE = 0
+FI_CONTRIB_GOELZER = 1
+#: A_OCEAN_PD, present-day ocean surface (m^2), src/barystatic_sealevel.jl:1
+A_OCEAN_PD = 3.625e14
 FI_EXEC_PERSIST = 0
 FI_EXEC_GRAPH = 1
 FI_EXEC_LOOP = 2
@@ -71,6 +83,10 @@ FIELDS = {
     "columnanom_load": 19,
     "columnanom_full": 20,
     "H_af": 21,
+    "maskgrounded": 22,
+    "maskocean": 23,
+    "H_water": 24,
+    "columnanom_seawater": 25,
 }
 
 #: Float64(1f-5): the reference passes reltol as a Float32 literal (src/simulation.jl:13)
@@ -114,6 +130,28 @@ class FiConfig(C.Structure):
         ("max_steps", C.c_int64),
         ("form", C.c_int32),
         ("device", C.c_int32),
+        ("sealevel_load", C.c_int32),
+        ("bsl_mode", C.c_int32),
+        ("bsl_update", C.c_int32),
+        ("volume_contribution", C.c_int32),
+        ("density_contribution", C.c_int32),
+        ("adjustment_contribution", C.c_int32),
+        ("bsl_ref_A", C.c_double),
+    ]
+
+
+class FiSealevel(C.Structure):
+    """``fi_sealevel`` (include/fastiso_b200.h)."""
+
+    _fields_ = [
+        ("z_bsl", C.c_double),
+        ("A_bsl", C.c_double),
+        ("V_af", C.c_double),
+        ("V_den", C.c_double),
+        ("V_pov", C.c_double),
+        ("delta_V", C.c_double),
+        ("tracked", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
@@ -169,6 +207,13 @@ def default_config(nx: int, ny: int, Wx: float, Wy: float) -> FiConfig:
     c.max_steps = 1_000_000
     c.form = FI_FORM_FP32
     c.device = 0
+    c.sealevel_load = FI_SEALEVEL_LOAD_NONE
+    c.bsl_mode = FI_BSL_CONSTANT
+    c.bsl_update = FI_BSL_UPDATE_INTERNAL
+    c.volume_contribution = FI_CONTRIB_GOELZER
+    c.density_contribution = FI_CONTRIB_GOELZER
+    c.adjustment_contribution = FI_CONTRIB_NONE
+    c.bsl_ref_A = A_OCEAN_PD
     return c
 
 
@@ -217,6 +262,10 @@ _SIGS = {
     "fi_get_step_record": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.POINTER(C.c_int64)]),
     "fi_set_step_replay": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]),
     "fi_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FiStats)]),
+    "fi_get_sealevel": (C.c_int, [C.c_void_p, C.POINTER(FiSealevel)]),
+    "fi_set_ocean_surface_table": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double),
+                                             C.POINTER(C.c_double)]),
+    "fi_set_bsl_history": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fi_checkpoint": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_size_t)]),
     "fi_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "fi_time_kernels": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),

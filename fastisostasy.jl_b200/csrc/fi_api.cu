@@ -47,6 +47,7 @@ struct PlainBufs {
     double *rhs, *bxx, *byy, *bx, *bxy, *Mxx, *Myy, *Mxy, *buf, *cropped, *off, *partial;
     double2 *fftrhs, *P;
     double *D, *eta, *mask, *u_ref, *ue_ref, *z_b_ref, *z_ss_ref, *H_af_ref, *H_tab;
+    double *s_sw, *mgr, *moc, *hwater;  // seawater anomaly, masks, water column
     double2 *Ge_hat, *Gg_hat;
 };
 
@@ -115,6 +116,8 @@ struct fi_handle {
     size_t smem_cap = 0;
     double last_rhs_t = 0.0;
     long long nf_plain = 0;
+    // sea level: tables of PiecewiseConstantBSL (z -> A) and ImposedBSL (t -> z)
+    std::vector<double> osurf_z, osurf_A, bslh_t, bslh_z;
     // step-sequence record / replay buffers (FP32 form: device, plain form: host)
     double* d_rec = nullptr;
     double* d_replay = nullptr;
@@ -266,6 +269,13 @@ void fi_config_default(fi_config* c, int32_t nx, int32_t ny, double Wx, double W
     c->dt_sparse_diagnostics = 10.0;
     c->max_steps = 1000000;
     c->form = FI_FORM_FP32;
+    c->sealevel_load = FI_SEALEVEL_LOAD_NONE;
+    c->bsl_mode = FI_BSL_CONSTANT;
+    c->bsl_update = FI_BSL_UPDATE_INTERNAL;
+    c->volume_contribution = FI_CONTRIB_GOELZER;
+    c->density_contribution = FI_CONTRIB_GOELZER;
+    c->adjustment_contribution = FI_CONTRIB_NONE;
+    c->bsl_ref_A = 3.625e14;  // A_OCEAN_PD, src/barystatic_sealevel.jl:1
 }
 
 const char* fi_status_string(int32_t s) {
@@ -422,6 +432,10 @@ static int create_buffers(fi_handle* h) {
         RET(dalloc(h, &ueref, n)); m.ue_ref = ueref;
         RET(dalloc(h, &Hext, n)); m.H_ext = Hext;
         RET(dalloc(h, &m.dz, n));
+        RET(dalloc(h, &m.sw, n));
+        RET(dalloc(h, &m.mgr, n));
+        RET(dalloc(h, &m.moc, n));
+        RET(dalloc(h, &m.hwater, n));
         RET(dalloc(h, &m.sig_load, n));
         RET(dalloc(h, &m.sig_geo, n));
         RET(dalloc(h, &m.S[0], (size_t)h->ny * h->sp));
@@ -482,11 +496,11 @@ static int create_buffers(fi_handle* h) {
                            &p.now_u, &p.ue, &p.dz, &p.H, &p.H_af, &p.z_b, &p.z_ss, &p.s_i, &p.s_l, &p.s_m,
                            &p.s_load, &p.s_full, &p.dudt, &p.rhs, &p.bxx, &p.byy, &p.bx, &p.bxy, &p.Mxx,
                            &p.Myy, &p.Mxy, &p.buf, &p.D, &p.eta, &p.mask, &p.u_ref, &p.ue_ref, &p.z_b_ref,
-                           &p.z_ss_ref, &p.H_af_ref};
+                           &p.z_ss_ref, &p.H_af_ref, &p.s_sw, &p.mgr, &p.moc, &p.hwater};
         for (double** b : bufs) RET(dalloc(h, b, n));
         RET(dalloc(h, &p.cropped, (size_t)(2 * h->nx - 1) * (2 * h->ny - 1)));
         RET(dalloc(h, &p.off, 4));
-        RET(dalloc(h, &p.partial, 2 * (size_t)h->red_blocks));
+        RET(dalloc(h, &p.partial, 3 * (size_t)h->red_blocks));
         RET(dalloc(h, &p.fftrhs, n));
         RET(dalloc(h, &p.P, M));
         RET(dalloc(h, &p.Ge_hat, M));
@@ -598,6 +612,20 @@ extern "C" int fi_set_field(fi_handle* h, int32_t field, const double* host, siz
     if (h) cudaSetDevice(h->cfg.device);
     if (!h || !host) return FI_ERR_ARG;
     if (n != N2(h)) return set_err(h, FI_ERR_ARG, "field size %zu != nx*ny", n);
+    if (field == FI_FIELD_U && h->initialized) {
+        // integrator.u .= host, as a coupling callback does: copied straight from the
+        // caller's buffer (pinned memory makes it one DMA); the next step re-evaluates
+        // the FSAL derivative at the new state (u_modified!)
+        if (h->cfg.form == FI_FORM_FP32) {
+            RET(read_ctl(h));
+            CK(cudaMemcpyAsync(h->mem.u[h->ctl.ibuf], host, n * 8, cudaMemcpyHostToDevice, h->stream));
+        } else {
+            CK(cudaMemcpyAsync(h->p.u[h->ctl.ibuf], host, n * 8, cudaMemcpyHostToDevice, h->stream));
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->integ_started) h->fsal_pending = true;
+        return FI_OK;
+    }
     std::vector<double> v(host, host + n);
     switch (field) {
         case FI_FIELD_LITHO_RIGIDITY: h->D = v; return FI_OK;
@@ -608,16 +636,7 @@ extern "C" int fi_set_field(fi_handle* h, int32_t field, const double* host, siz
         case FI_FIELD_UE_REF: h->ue_ref = v; return FI_OK;
         case FI_FIELD_DZ_SS_REF: h->dz_ss_ref = v; return FI_OK;
         case FI_FIELD_Z_B_REF: h->z_b_ref = v; return FI_OK;
-        case FI_FIELD_U:
-            if (!h->initialized) { h->u_init = v; h->u_set = true; return FI_OK; }
-            if (h->cfg.form == FI_FORM_FP32) {
-                RET(read_ctl(h));
-                CK(cudaMemcpyAsync(h->mem.u[h->ctl.ibuf], host, n * 8, cudaMemcpyHostToDevice, h->stream));
-            } else {
-                CK(cudaMemcpyAsync(h->p.u[h->ctl.ibuf], host, n * 8, cudaMemcpyHostToDevice, h->stream));
-            }
-            CK(cudaStreamSynchronize(h->stream));
-            return FI_OK;
+        case FI_FIELD_U: h->u_init = v; h->u_set = true; return FI_OK;
         case FI_FIELD_H_ICE:
             if (h->cfg.ice_mode != FI_ICE_EXTERNAL)
                 return set_err(h, FI_ERR_ARG, "H_ice is set externally only with FI_ICE_EXTERNAL");
@@ -635,6 +654,27 @@ extern "C" int fi_set_ice_history(fi_handle* h, int32_t K, const double* t, cons
     h->ice_t.assign(t, t + K);
     h->ice_H.assign(H, H + (size_t)K * N2(h));
     return FI_OK;
+}
+
+static int set_table(fi_handle* h, int32_t n, const double* x, const double* y, std::vector<double>& xo,
+                     std::vector<double>& yo) {
+    if (n < 2 || !x || !y) return set_err(h, FI_ERR_ARG, "a table needs >= 2 points");
+    for (int k = 1; k < n; k++)
+        if (!(x[k] > x[k - 1])) return set_err(h, FI_ERR_ARG, "table abscissae must increase");
+    if (h->initialized) return set_err(h, FI_ERR_STATE, "tables are set before fi_init");
+    xo.assign(x, x + n);
+    yo.assign(y, y + n);
+    return FI_OK;
+}
+
+extern "C" int fi_set_ocean_surface_table(fi_handle* h, int32_t n, const double* z, const double* A) {
+    if (!h) return FI_ERR_ARG;
+    return set_table(h, n, z, A, h->osurf_z, h->osurf_A);
+}
+
+extern "C" int fi_set_bsl_history(fi_handle* h, int32_t n, const double* t, const double* z) {
+    if (!h) return FI_ERR_ARG;
+    return set_table(h, n, t, z, h->bslh_t, h->bslh_z);
 }
 
 extern "C" int fi_set_elastic_table(fi_handle* h, int32_t n, const double* rm, const double* GE) {
@@ -733,6 +773,27 @@ extern "C" int fi_init(fi_handle* h) {
         return set_err(h, FI_ERR_STATE, "ice history not set");
     const bool elastic = c.lithosphere != FI_LITHO_RIGID, geoid = c.sea_surface == FI_SEA_SURFACE_LATERALLY_VARIABLE;
     if (elastic && h->rm.size() < 2) return set_err(h, FI_ERR_STATE, "elastic Green table not set");
+    if (c.sealevel_load != FI_SEALEVEL_LOAD_NONE && c.sealevel_load != FI_SEALEVEL_LOAD_INTERACTIVE)
+        return set_err(h, FI_ERR_ARG, "unknown sea-level load %d", c.sealevel_load);
+    if (c.bsl_mode < FI_BSL_CONSTANT || c.bsl_mode > FI_BSL_IMPOSED)
+        return set_err(h, FI_ERR_ARG, "unknown BSL %d", c.bsl_mode);
+    const bool bsl_internal = c.bsl_update == FI_BSL_UPDATE_INTERNAL;
+    if (bsl_internal && c.bsl_mode == FI_BSL_PIECEWISE_CONSTANT && h->osurf_z.size() < 2)
+        return set_err(h, FI_ERR_STATE, "PiecewiseConstantBSL needs fi_set_ocean_surface_table");
+    if (bsl_internal && c.bsl_mode == FI_BSL_IMPOSED && h->bslh_t.size() < 2)
+        return set_err(h, FI_ERR_STATE, "ImposedBSL needs fi_set_bsl_history");
+    if (c.form == FI_FORM_FP32 && bsl_internal &&
+        (c.bsl_mode == FI_BSL_CONSTANT_OCEAN_SURFACE || c.bsl_mode == FI_BSL_PIECEWISE_CONSTANT))
+        return set_err(h, FI_ERR_UNSUPPORTED,
+                       "a BSL driven by the ice volume runs in the plain FP64 form (the FP32 form's sparse update "
+                       "does not sum the volumes)");
+    if (c.sealevel_load == FI_SEALEVEL_LOAD_INTERACTIVE) {
+        size_t active = 0;
+        for (size_t k = 0; k < n; k++) active += h->mask[k] != 0.0;
+        if ((double)active > 0.6 * (double)n)
+            return set_err(h, FI_ERR_ARG, "Mask defining regions of active load must not cover more than 60%% of "
+                                          "the cells when using an interactive sea level.");
+    }
     // spectral factors and Green's functions, FP64 on the device
     double *d_ratio = nullptr, *d_thick = nullptr, *d_Rg = nullptr;
     const int nch = (int)h->ch_ratio.size();
@@ -772,9 +833,23 @@ extern "C" int fi_init(fi_handle* h) {
     h->z_ss_ref.resize(n);
     h->H_af_ref.resize(n);
     const double rsi = c.rho_seawater / c.rho_ice;
+    // ReferenceState masks and water column (CurrentState copies them) and the volumes
+    // of init_problem! (src/simulation.jl:132-151, 305-312)
+    std::vector<double> mgr0(n), moc0(n), hw0(n);
+    double saf = 0.0, sden = 0.0, spov = 0.0;
     for (size_t k = 0; k < n; k++) {
         h->z_ss_ref[k] = c.z_bsl + h->dz_ss_ref[k];
         h->H_af_ref[k] = haf_host(rsi, h->H_ice_ref[k], h->z_b_ref[k], h->z_ss_ref[k]);
+        const bool gr = h->H_af_ref[k] > 0;
+        const double w = h->z_ss_ref[k] - h->z_b_ref[k];
+        const bool oc = w > 0 && !gr;
+        const double wc = w > 0 ? w : 0.0, H = h->H_ice_ref[k];
+        mgr0[k] = gr;
+        moc0[k] = oc;
+        hw0[k] = (H <= 1 ? wc : 0.0) + ((!gr && H > 1) ? wc - H * (c.rho_ice / c.rho_seawater) : 0.0);
+        saf += h->H_af_ref[k] * h->dx * h->dy;
+        sden += H * h->dx * h->dy;
+        spov += wc * h->dx * h->dy;
     }
     std::vector<double> u0 = h->u_set ? h->u_init : h->u_ref;
     Ctl& ct = h->ctl;
@@ -787,6 +862,12 @@ extern "C" int fi_init(fi_handle* h) {
     ct.max_steps = c.max_steps;
     ct.active = 1;
     ct.t_stop = c.t1;
+    ct.z_bsl = c.z_bsl;
+    ct.A_bsl = c.bsl_ref_A;
+    ct.V_af = c.volume_contribution == FI_CONTRIB_GOELZER ? saf * c.rho_ice / c.rho_seawater : 0.0;
+    ct.V_den = c.density_contribution == FI_CONTRIB_GOELZER
+                   ? sden * (c.rho_ice / c.rho_water - c.rho_ice / c.rho_seawater) : 0.0;
+    ct.V_pov = c.adjustment_contribution == FI_CONTRIB_GOELZER ? spov : 0.0;
     if (c.form == FI_FORM_FP32) {
         const int K = (int)h->ice_t.size();
         Member& m = h->mem;
@@ -799,6 +880,23 @@ extern "C" int fi_init(fi_handle* h) {
         m.column_compressible = c.lithosphere_column == FI_COLUMN_COMPRESSIBLE;
         m.ice_external = c.ice_mode == FI_ICE_EXTERNAL;
         m.ice_flat = c.ice_flat_bc;
+        m.sl_interactive = c.sealevel_load == FI_SEALEVEL_LOAD_INTERACTIVE;
+        m.bsl_imposed = bsl_internal && c.bsl_mode == FI_BSL_IMPOSED;
+        m.bsl_ref_z = c.z_bsl;
+        m.rho_sw = c.rho_seawater;
+        if (m.bsl_imposed) {
+            double *bt, *bz;
+            RET(dalloc(h, &bt, h->bslh_t.size()));
+            RET(dalloc(h, &bz, h->bslh_z.size()));
+            RET(upload(h, bt, h->bslh_t));
+            RET(upload(h, bz, h->bslh_z));
+            m.bslh_t = bt;
+            m.bslh_z = bz;
+            m.n_bslh = (int)h->bslh_t.size();
+        }
+        RET(upload(h, m.mgr, mgr0));
+        RET(upload(h, m.moc, moc0));
+        RET(upload(h, m.hwater, hw0));
         // FP32 parameter maps
         std::vector<double> vf(n), sigref(n), zbss(n);
         bool any_mask = false, any_haf = false, any_sig = false, any_ueref = false, zb_uniform = true;
@@ -876,6 +974,9 @@ extern "C" int fi_init(fi_handle* h) {
         RET(upload(h, p.H_af, h->H_af_ref));
         RET(upload(h, p.z_b, h->z_b_ref));
         RET(upload(h, p.z_ss, h->z_ss_ref));
+        RET(upload(h, p.mgr, mgr0));
+        RET(upload(h, p.moc, moc0));
+        RET(upload(h, p.hwater, hw0));
         if (elastic) RET(build_kernel_spectrum(h, h->d_Ge, nullptr, p.Ge_hat));
         if (geoid) RET(build_kernel_spectrum(h, h->d_Gg, nullptr, p.Gg_hat));
         RET(rhs_plain(h, c.t0, p.u[0], p.fscratch));
@@ -1027,6 +1128,8 @@ static int conv_plain(fi_handle* h, const double* input, const double2* Ghat, do
 }
 
 // update_diagnostics!(dudt, u, sim, t), one kernel per broadcast of the reference
+static int reduce_host(fi_handle* h, const double* d_partial, int nblk, int stride, double* out);
+
 static int rhs_plain(fi_handle* h, double t, double* u, double* dudt) {
     const fi_config& c = h->cfg;
     PlainBufs& p = h->p;
@@ -1073,19 +1176,44 @@ static int rhs_plain(fi_handle* h, double t, double* u, double* dudt) {
         }
         kp_litho<<<g, NT, 0, h->stream>>>(p.ue, p.ue_ref, p.s_l, c.rho_litho, n);
         CKL();
+        {
+            // internal_update_bsl! (src/sealevel.jl:242-262): the volumes on the first
+            // H_af of this call, the old z_ss and the current z_b, then update_bsl!
+            Ctl& ct = h->ctl;
+            kp_volumes<<<h->red_blocks, NT, 0, h->stream>>>(p.H_af, p.H, p.z_ss, p.z_b, h->dx * h->dy, p.partial, n);
+            CKL();
+            double v3[3] = {0.0, 0.0, 0.0};
+            RET(reduce_host(h, p.partial, h->red_blocks, 3, v3));
+            const double Vold = ct.V_af + ct.V_den + ct.V_pov;
+            ct.V_af = c.volume_contribution == FI_CONTRIB_GOELZER ? v3[0] * c.rho_ice / c.rho_seawater : 0.0;
+            ct.V_den = c.density_contribution == FI_CONTRIB_GOELZER
+                           ? v3[1] * (c.rho_ice / c.rho_water - c.rho_ice / c.rho_seawater) : 0.0;
+            ct.V_pov = c.adjustment_contribution == FI_CONTRIB_GOELZER ? v3[2] : 0.0;
+            ct.delta_V = (ct.V_af + ct.V_den + ct.V_pov) - Vold;
+            if (c.bsl_update == FI_BSL_UPDATE_INTERNAL) {
+                const int st = bsl_update(&ct, c.bsl_mode, c.z_bsl, c.bsl_ref_A, -ct.delta_V, t, h->osurf_z.data(),
+                                          h->osurf_A.data(), (int)h->osurf_z.size(), h->bslh_t.data(),
+                                          h->bslh_z.data(), (int)h->bslh_t.size());
+                if (st) return set_err(h, st, "update_bsl!: BSL %.6g or t = %.6g outside its table", ct.z_bsl, t);
+            }
+        }
         if (c.sea_surface == FI_SEA_SURFACE_LATERALLY_VARIABLE) {
             kp_geo_in<<<g, NT, 0, h->stream>>>(p.s_load, p.s_full, p.s_m, p.mask,
                                               c.lithosphere_column == FI_COLUMN_COMPRESSIBLE, h->dx * h->dy, p.buf, n);
             CKL();
             RET(conv_plain(h, p.buf, p.Gg_hat, c.bc_sea_surface_border, p.dz));
         }
-        kp_zss<<<g, NT, 0, h->stream>>>(p.z_ss_ref, p.dz, c.z_bsl, p.z_ss, n);
+        kp_zss<<<g, NT, 0, h->stream>>>(p.z_ss_ref, p.dz, h->ctl.z_bsl, p.z_ss, n);
         CKL();
         kp_haf_ice<<<g, NT, 0, h->stream>>>(p.H, p.z_b, p.z_ss, p.H_af_ref, p.H_af, p.s_i, rsi, c.rho_ice, n);
         CKL();
+        kp_sealevel<<<g, NT, 0, h->stream>>>(p.H, p.H_af, p.z_ss, p.z_b, p.z_ss_ref, p.mask,
+                                             c.sealevel_load == FI_SEALEVEL_LOAD_INTERACTIVE, c.rho_seawater,
+                                             c.rho_ice / c.rho_seawater, p.mgr, p.moc, p.hwater, p.s_sw, n);
+        CKL();
         h->ctl.count_sparse += 1;
     }
-    kp_load_full<<<g, NT, 0, h->stream>>>(p.s_i, p.s_l, p.s_m, p.mask, p.s_load, p.s_full, n);
+    kp_load_full<<<g, NT, 0, h->stream>>>(p.s_i, p.s_sw, p.s_l, p.s_m, p.mask, p.s_load, p.s_full, n);
     CKL();
     kp_rhs_init<<<g, NT, 0, h->stream>>>(p.s_full, c.g, p.rhs, n);
     CKL();
@@ -2085,6 +2213,29 @@ extern "C" int fi_ensemble_trace(fi_ensemble* e, int32_t on, double* ms, int64_t
     return FI_OK;
 }
 
+extern "C" int fi_get_sealevel(fi_handle* h, fi_sealevel* out) {
+    if (h) cudaSetDevice(h->cfg.device);
+    if (!h || !out) return FI_ERR_ARG;
+    memset(out, 0, sizeof(*out));
+    if (!h->initialized) {
+        out->z_bsl = h->cfg.z_bsl;
+        out->A_bsl = h->cfg.bsl_ref_A;
+        return FI_OK;
+    }
+    RET(read_ctl(h));
+    const Ctl& ct = h->ctl;
+    out->z_bsl = ct.z_bsl;
+    out->A_bsl = ct.A_bsl;
+    out->tracked = h->cfg.form == FI_FORM_FP64;
+    if (out->tracked) {
+        out->V_af = ct.V_af;
+        out->V_den = ct.V_den;
+        out->V_pov = ct.V_pov;
+        out->delta_V = ct.delta_V;
+    }
+    return FI_OK;
+}
+
 extern "C" int fi_get_stats(fi_handle* h, fi_stats* st) {
     if (h) cudaSetDevice(h->cfg.device);
     if (!h || !st) return FI_ERR_ARG;
@@ -2221,6 +2372,10 @@ extern "C" int fi_get_field(fi_handle* h, int32_t field, double* host, size_t n)
                     case FI_FIELD_COLUMNANOM_LOAD: src = p.s_load; break;
                     case FI_FIELD_COLUMNANOM_FULL: src = p.s_full; break;
                     case FI_FIELD_H_AF: src = p.H_af; break;
+                    case FI_FIELD_MASKGROUNDED: src = p.mgr; break;
+                    case FI_FIELD_MASKOCEAN: src = p.moc; break;
+                    case FI_FIELD_H_WATER: src = p.hwater; break;
+                    case FI_FIELD_COLUMNANOM_SEAWATER: src = p.s_sw; break;
                     default: return set_err(h, FI_ERR_ARG, "unknown field %d", field);
                 }
                 RET(download(h, v, src, n));
@@ -2259,8 +2414,12 @@ extern "C" int fi_get_field(fi_handle* h, int32_t field, double* host, size_t n)
                 }
                 case FI_FIELD_Z_SS:
                     v.resize(n);
-                    for (size_t k = 0; k < n; k++) v[k] = h->z_ss_ref[k] + dz[k] + c.z_bsl;
+                    for (size_t k = 0; k < n; k++) v[k] = h->z_ss_ref[k] + dz[k] + ct.z_bsl;
                     break;
+                case FI_FIELD_MASKGROUNDED: RET(download(h, v, m.mgr, n)); break;
+                case FI_FIELD_MASKOCEAN: RET(download(h, v, m.moc, n)); break;
+                case FI_FIELD_H_WATER: RET(download(h, v, m.hwater, n)); break;
+                case FI_FIELD_COLUMNANOM_SEAWATER: RET(download(h, v, m.sw, n)); break;
                 case FI_FIELD_COLUMNANOM_LOAD: RET(download(h, v, m.sig_load, n)); break;
                 case FI_FIELD_COLUMNANOM_FULL:
                     if (m.column_compressible) return set_err(h, FI_ERR_UNSUPPORTED, "full anomaly not kept");

@@ -19,6 +19,49 @@ __host__ __device__ inline double dtmin_at(double dtmin, double t) {
     return dtmin > e ? dtmin : e;
 }
 
+// interpolate(x, ::TimeInterpolation0D) with flat_bc = false (src/interpolations.jl:20-40):
+// linear inside [xs[0], xs[n-1]], FI_ERR_FORCING_RANGE outside.
+__host__ __device__ inline int interp0d(const double* xs, const double* ys, int n, double x, double* y) {
+    if (n < 2 || !(x >= xs[0]) || x > xs[n - 1]) return FI_ERR_FORCING_RANGE;
+    int lo = 0, hi = n - 1;  // last index with xs[lo] <= x, lo < n - 1
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (xs[mid] <= x) lo = mid; else hi = mid;
+    }
+    const double w = (x - xs[lo]) / (xs[lo + 1] - xs[lo]);
+    *y = ys[lo] + w * (ys[lo + 1] - ys[lo]);
+    return FI_OK;
+}
+
+// update_bsl!(bsl, -delta_V, t) of each BSL (src/barystatic_sealevel.jl:215-235) on the
+// control block's z_bsl / A_bsl; dV = -delta_V.  Tables: the ocean surface A(z) of
+// PiecewiseConstantBSL, the history z(t) of ImposedBSL.
+__host__ __device__ inline int bsl_update(Ctl* c, int mode, double ref_z, double ref_A, double dV, double t,
+                                          const double* oz, const double* oA, int no, const double* ht,
+                                          const double* hz, int nh) {
+    switch (mode) {
+        case FI_BSL_CONSTANT: c->z_bsl = ref_z; return FI_OK;
+        case FI_BSL_CONSTANT_OCEAN_SURFACE:
+            c->A_bsl = ref_A;
+            c->z_bsl += dV / c->A_bsl;
+            return FI_OK;
+        case FI_BSL_PIECEWISE_CONSTANT: {
+            c->z_bsl += dV / c->A_bsl;
+            double A;
+            const int st = interp0d(oz, oA, no, c->z_bsl, &A);
+            if (st == FI_OK) c->A_bsl = A;
+            return st;
+        }
+        case FI_BSL_IMPOSED: {
+            double z;
+            const int st = interp0d(ht, hz, nh, t, &z);
+            if (st == FI_OK) c->z_bsl = z;
+            return st;
+        }
+        default: return FI_ERR_ARG;
+    }
+}
+
 // Sparse-update gate of update_diagnostics!: (t - t0)/dt_sparse >= count
 // (src/simulation.jl:355-356).  When it fires, the elastic displacement of this
 // call goes to the other ue buffer while z_b still reads the old one (the
@@ -29,6 +72,13 @@ __device__ inline int gate_eval(const Member& m, Ctl* c, double t_rhs) {
     if (g) {
         c->count_sparse += 1;
         c->iue ^= 1;
+        // internal_update_bsl! of an ImposedBSL: z_bsl(t) (the volume-driven BSLs run in
+        // the plain form, which sums the volumes first)
+        if (m.bsl_imposed) {
+            double z;
+            if (interp0d(m.bslh_t, m.bslh_z, m.n_bslh, t_rhs, &z) == FI_OK) c->z_bsl = z;
+            else c->status = FI_ERR_FORCING_RANGE;
+        }
     }
     c->gate = g;
     return g;

@@ -64,6 +64,9 @@ struct Ctl {
     const double* replay_dt;
     double* rec_dt;
     long long replay_n, replay_i, rec_cap, rec_n;
+    // barystatic sea level and ocean area (sim.now.z_bsl, sim.sealevel.bsl.A) and the
+    // volume terms of the last sparse update (V_af, V_den, V_pov, delta_V)
+    double z_bsl, A_bsl, V_af, V_den, V_pov, delta_V;
 };
 
 // Shared-memory layout of the forward row phase: byte offsets (16-byte aligned) of the
@@ -134,6 +137,20 @@ struct Member {
     double* cpart;              // corner partials [ncols][4] of the last column pass
     const double* tout;         // output times (nout_condition), ctl->nout entries
     Ctl* ctl;
+    // sea level beyond the surface (src/loads.jl:56-85, src/topography.jl:1-28): the
+    // seawater column anomaly of InteractiveSealevelLoad and the masks / water column
+    // of the last sparse update; an ImposedBSL history
+    int sl_interactive;         // sealevel.load isa InteractiveSealevelLoad
+    int bsl_imposed;            // z_bsl(t) from bslh_t / bslh_z at each sparse update
+    int n_bslh, pad_sl;
+    double bsl_ref_z;           // ReferenceBSL z (the z_bsl folded into zbss_ref)
+    double rho_sw;              // seawater density
+    const double* bslh_t;
+    const double* bslh_z;
+    float* sw;                  // columnanoms.seawater
+    float* mgr;                 // maskgrounded (0/1)
+    float* moc;                 // maskocean (0/1)
+    float* hwater;              // H_water
 };
 
 enum {

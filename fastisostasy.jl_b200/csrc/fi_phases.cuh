@@ -264,6 +264,9 @@ struct FwdScalars {
     double a1, a2, a3, c1, c2, c3, off;  // stage combination and the stage vector's corner offset
     double cue, cuz, cdz;                // corner offsets of ue (current, for z_b) and of dz
     double w;                            // ice interpolation weight
+    double dzbsl, zbsl;                  // z_bsl - ReferenceBSL z, and z_bsl
+    int gated;                           // this call ran the sparse update
+    int pad_g;
     const double* uprev;
     double* unew;                        // where the boundary-corrected stage vector goes (or null)
     int ice_i, iue, iuz, ik;
@@ -287,6 +290,9 @@ __device__ inline void fwd_static(const Member& m, const Ctl& c, int stage, cons
     s.cdz = cmean(c.dz_corner, m.border_g);
     s.iue = c.iue;
     s.iuz = c.iue_zb;
+    s.dzbsl = c.z_bsl - m.bsl_ref_z;
+    s.zbsl = c.z_bsl;
+    s.gated = c.gate;
     s.stage = stage;
     s.ik = c.ik;
     s.uprev = (stage == 0) ? uin : m.u[c.ibuf];
@@ -491,14 +497,32 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
             const float ha = v.Ha[i];
             const double H = (double)(fw != 0.0f ? ha + (v.Hb[i] - ha) * fw : ha);
             const double uev = (double)v.ue[i] - cue;
+            const double dzv = (double)v.dz[i] - cdz;
             const double zdiff = (double)((flags & FLAG_ZBSS) ? v.zbss[i] : m.zbss_scalar) +
-                                 ((double)v.uz[i] - cuz) + u - ((double)v.dz[i] - cdz);
+                                 ((double)v.uz[i] - cuz) + u - dzv - s.dzbsl;
             double haf = H + (zdiff < 0.0 ? zdiff : 0.0) * m.rho_sw_ice;
             haf = haf > 0.0 ? haf : 0.0;
             const double mk = (flags & FLAG_MASK) ? (double)v.mask[i] : 1.0;
             const double hafref = (flags & FLAG_HAFREF) ? (double)v.hafref[i] : 0.0;
-            const double sload = mk * (m.rho_ice * (haf - hafref));
-            double sfull = mk * (m.rho_ice * haf + m.rho_litho * uev + m.rho_um * u);
+            double ssw = 0.0;
+            if (s.gated) {
+                // update_maskgrounded!, update_maskocean!, watercolumn!, columnanom_water!
+                // (src/topography.jl:1-28, src/loads.jl:56-85) after the sparse update
+                const bool gr = haf > 0.0;
+                const double w = -zdiff;  // z_ss - z_b
+                const bool oc = w > 0.0 && !gr;
+                const double wc = w > 0.0 ? w : 0.0;
+                const double hw = (H <= 1.0 ? wc : 0.0) + ((!gr && H > 1.0) ? wc - H / m.rho_sw_ice : 0.0);
+                if (m.sl_interactive && oc) ssw = m.rho_sw * (dzv + s.zbsl) * mk;
+                m.sw[g] = (float)ssw;
+                m.mgr[g] = gr ? 1.0f : 0.0f;
+                m.moc[g] = oc ? 1.0f : 0.0f;
+                m.hwater[g] = (float)hw;
+            } else if (m.sl_interactive) {
+                ssw = (double)m.sw[g];
+            }
+            const double sload = mk * (m.rho_ice * (haf - hafref) + ssw);
+            double sfull = mk * (m.rho_ice * haf + m.rho_litho * uev + m.rho_um * u + ssw);
             if (flags & FLAG_SIGREF) sfull -= (double)v.sigref[i];
             m.sig_load[g] = (float)sload;
             double geo = sfull;

@@ -65,12 +65,47 @@ __global__ void kp_zss(const double* z_ss_ref, const double* dz, double z_bsl, d
     GRID_STRIDE(i, n) z_ss[i] = z_ss_ref[i] + dz[i] + z_bsl;
 }
 
-__global__ void kp_load_full(const double* s_i, const double* s_l, const double* s_m, const double* mask,
-                             double* s_load, double* s_full, size_t n) {
+__global__ void kp_load_full(const double* s_i, const double* s_sw, const double* s_l, const double* s_m,
+                             const double* mask, double* s_load, double* s_full, size_t n) {
     GRID_STRIDE(i, n) {
-        const double ld = mask[i] * (s_i[i] + 0.0 + 0.0);  // seawater and sediment anomalies are zero
+        const double ld = mask[i] * (s_i[i] + s_sw[i] + 0.0);  // the sediment anomaly is zero
         s_load[i] = ld;
         s_full[i] = ld + mask[i] * (s_l[i] + s_m[i]);
+    }
+}
+
+// block partial sums of H_af A, H_ice A and max(z_ss - z_b, 0) A (update_V_af!,
+// update_V_den!, update_V_pov!, src/sealevel.jl:275-332), three per block
+__global__ void kp_volumes(const double* H_af, const double* H, const double* z_ss, const double* z_b, double A,
+                           double* partial, size_t n) {
+    __shared__ double red[96];
+    double a = 0.0, d = 0.0, p = 0.0;
+    GRID_STRIDE(i, n) {
+        a += H_af[i] * A;
+        d += H[i] * A;
+        const double w = z_ss[i] - z_b[i];
+        p += (w > 0 ? w : 0.0) * A;
+    }
+    double v[3] = {a, d, p};
+    block_sum<3>(v, red);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; q++) partial[3 * blockIdx.x + q] = v[q];
+}
+
+// update_maskgrounded!, update_maskocean!, watercolumn! and columnanom_water!
+// (src/topography.jl:1-28, src/loads.jl:56-85)
+__global__ void kp_sealevel(const double* H, const double* H_af, const double* z_ss, const double* z_b,
+                            const double* z_ss_ref, const double* mask, int interactive, double rho_sw,
+                            double rho_i_sw, double* mgr, double* moc, double* hwater, double* s_sw, size_t n) {
+    GRID_STRIDE(i, n) {
+        const bool gr = H_af[i] > 0;
+        const double w = z_ss[i] - z_b[i];
+        const bool oc = w > 0 && !gr;
+        const double wc = w > 0 ? w : 0.0;
+        mgr[i] = gr;
+        moc[i] = oc;
+        hwater[i] = (H[i] <= 1 ? wc : 0.0) + ((!gr && H[i] > 1) ? wc - H[i] * rho_i_sw : 0.0);
+        s_sw[i] = interactive ? rho_sw * (z_ss[i] - z_ss_ref[i]) * (oc ? 1.0 : 0.0) * mask[i] : 0.0;
     }
 }
 

@@ -15,8 +15,13 @@ __global__ void kp_litho(const double* ue, const double* ue_ref, double* s_l, do
 __global__ void kp_geo_in(const double* s_load, const double* s_full, const double* s_m, const double* mask,
                           int compressible, double A, double* out, size_t n);
 __global__ void kp_zss(const double* z_ss_ref, const double* dz, double z_bsl, double* z_ss, size_t n);
-__global__ void kp_load_full(const double* s_i, const double* s_l, const double* s_m, const double* mask,
-                             double* s_load, double* s_full, size_t n);
+__global__ void kp_load_full(const double* s_i, const double* s_sw, const double* s_l, const double* s_m,
+                             const double* mask, double* s_load, double* s_full, size_t n);
+__global__ void kp_volumes(const double* H_af, const double* H, const double* z_ss, const double* z_b, double A,
+                           double* partial, size_t n);
+__global__ void kp_sealevel(const double* H, const double* H_af, const double* z_ss, const double* z_b,
+                            const double* z_ss_ref, const double* mask, int interactive, double rho_sw,
+                            double rho_i_sw, double* mgr, double* moc, double* hwater, double* s_sw, size_t n);
 __global__ void kp_rhs_init(const double* s_full, double g, double* rhs, size_t n);
 __global__ void kp_dxx(double* du, const double* u, int nx, int ny, double Dx);
 __global__ void kp_dyy(double* du, const double* u, int nx, int ny, double Dy);

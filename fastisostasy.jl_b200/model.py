@@ -64,6 +64,13 @@ class LaterallyVariableSeaSurface(_Tag): pass
 class NoSealevelLoad(_Tag): pass
 class InteractiveSealevelLoad(_Tag): pass
 class InternalBSLUpdate(_Tag): pass
+class ExternalBSLUpdate(_Tag): pass
+class NoVolumeContribution(_Tag): pass
+class GoelzerVolumeContribution(_Tag): pass
+class NoDensityContribution(_Tag): pass
+class GoelzerDensityContribution(_Tag): pass
+class NoAdjustmentContribution(_Tag): pass
+class GoelzerAdjustmentContribution(_Tag): pass
 class RegularBCSpace(_Tag): pass
 class ExtendedBCSpace(_Tag): pass
 
@@ -74,13 +81,50 @@ class SeakonCalibration:
 
 
 @dataclass
-class ConstantBSL:
-    """ConstantBSL with a ReferenceBSL stub: z = 0 and A = A_OCEAN_PD
-    (src/barystatic_sealevel.jl:1, 100-110); the reference downloads the ocean
-    surface table to build ReferenceBSL, which this path never reads."""
+class ReferenceBSL:
+    """ReferenceBSL(z) (src/barystatic_sealevel.jl:3-42): the reference level z, its
+    ocean area A and the table A(z) of PiecewiseConstantBSL.  The reference downloads
+    the ocean-surface table; here the caller supplies it (z_vec, A_vec, already
+    unbiased so that A(0) = A_OCEAN_PD) when a BSL needs it, and A defaults to
+    A_OCEAN_PD, its value at z = 0."""
 
     z: float = 0.0
     A: float = 3.625e14
+    z_vec: list | None = None
+    A_vec: list | None = None
+
+
+@dataclass
+class ConstantBSL:
+    """ConstantBSL(; ref): z = ref.z for ever (src/barystatic_sealevel.jl:100-110, 215-218)."""
+
+    ref: ReferenceBSL = field(default_factory=ReferenceBSL)
+
+    @property
+    def z(self):
+        return self.ref.z
+
+    @property
+    def A(self):
+        return self.ref.A
+
+
+@dataclass
+class ConstantOceanSurfaceBSL(ConstantBSL):
+    """z += delta_V / ref.A at every sparse update (src/barystatic_sealevel.jl:220-224)."""
+
+
+@dataclass
+class PiecewiseConstantBSL(ConstantBSL):
+    """z += delta_V / A, then A = A(z) from ref's table (src/barystatic_sealevel.jl:226-230)."""
+
+
+@dataclass
+class ImposedBSL(ConstantBSL):
+    """z = z(t) linear in the given history (src/barystatic_sealevel.jl:172-181, 232-235)."""
+
+    t_vec: list = field(default_factory=list)
+    z_vec: list = field(default_factory=list)
 
 
 class UnsupportedError(NotImplementedError):
@@ -311,16 +355,32 @@ class BoundaryConditions:
 
 @dataclass
 class RegionalSeaLevel:
+    """RegionalSeaLevel (src/sealevel.jl:114-130) with the same keyword defaults."""
+
     surface: object = field(default_factory=LaterallyConstantSeaSurface)
     load: object = field(default_factory=NoSealevelLoad)
     bsl: ConstantBSL = field(default_factory=ConstantBSL)
     update_bsl: object = field(default_factory=InternalBSLUpdate)
+    volume_contribution: object = field(default_factory=GoelzerVolumeContribution)
+    density_contribution: object = field(default_factory=GoelzerDensityContribution)
+    adjustment_contribution: object = field(default_factory=NoAdjustmentContribution)
 
     def __post_init__(self):
-        if self.load != NoSealevelLoad():
-            raise UnsupportedError("InteractiveSealevelLoad is outside the LV-ELVA path")
+        if self.load not in (NoSealevelLoad(), InteractiveSealevelLoad()):
+            raise UnsupportedError(f"sea-level load {self.load!r}")
         if not isinstance(self.bsl, ConstantBSL):
-            raise UnsupportedError("only ConstantBSL is supported")
+            raise UnsupportedError(f"BSL {type(self.bsl).__name__} (PiecewiseLinearOceanSurfaceBSL needs NLsolve "
+                                   "and is not on the device path)")
+        if isinstance(self.bsl, PiecewiseConstantBSL) and self.bsl.ref.z_vec is None:
+            raise UnsupportedError("PiecewiseConstantBSL needs ReferenceBSL(z_vec, A_vec), the ocean-surface table")
+
+    @property
+    def bsl_mode(self):
+        for cls, mode in ((ImposedBSL, abi.FI_BSL_IMPOSED), (PiecewiseConstantBSL, abi.FI_BSL_PIECEWISE_CONSTANT),
+                          (ConstantOceanSurfaceBSL, abi.FI_BSL_CONSTANT_OCEAN_SURFACE)):
+            if isinstance(self.bsl, cls):
+                return mode
+        return abi.FI_BSL_CONSTANT
 
 
 @dataclass
@@ -409,6 +469,19 @@ class Simulation:
                            if sealevel.surface == LaterallyVariableSeaSurface()
                            else abi.FI_SEA_SURFACE_LATERALLY_CONSTANT)
         cfg.z_bsl = sealevel.bsl.z
+        cfg.bsl_ref_A = sealevel.bsl.A
+        cfg.sealevel_load = (abi.FI_SEALEVEL_LOAD_INTERACTIVE if sealevel.load == InteractiveSealevelLoad()
+                             else abi.FI_SEALEVEL_LOAD_NONE)
+        cfg.bsl_mode = sealevel.bsl_mode
+        cfg.bsl_update = (abi.FI_BSL_UPDATE_EXTERNAL if sealevel.update_bsl == ExternalBSLUpdate()
+                          else abi.FI_BSL_UPDATE_INTERNAL)
+        cfg.volume_contribution = (abi.FI_CONTRIB_NONE if sealevel.volume_contribution == NoVolumeContribution()
+                                   else abi.FI_CONTRIB_GOELZER)
+        cfg.density_contribution = (abi.FI_CONTRIB_NONE if sealevel.density_contribution == NoDensityContribution()
+                                    else abi.FI_CONTRIB_GOELZER)
+        cfg.adjustment_contribution = (abi.FI_CONTRIB_GOELZER
+                                       if sealevel.adjustment_contribution == GoelzerAdjustmentContribution()
+                                       else abi.FI_CONTRIB_NONE)
         cfg.bc_viscous_border = bcs.viscous_displacement.x_border
         cfg.bc_elastic_border = bcs.elastic_displacement.x_border
         cfg.bc_sea_surface_border = bcs.sea_surface_perturbation.x_border
@@ -459,6 +532,11 @@ class Simulation:
             "ice_H": self.ice_H,
             "elastic_table": self.elastic_table,
             "channels": (np.asarray(se.channel_ratio_means, float), np.asarray(se.channel_thickness_means, float)),
+            "ocean_surface": ((np.asarray(self.sealevel.bsl.ref.z_vec, float), np.asarray(self.sealevel.bsl.ref.A_vec,
+                                                                                         float))
+                              if self.sealevel.bsl.ref.z_vec is not None else None),
+            "bsl_history": ((np.asarray(self.sealevel.bsl.t_vec, float), np.asarray(self.sealevel.bsl.z_vec, float))
+                            if isinstance(self.sealevel.bsl, ImposedBSL) else None),
         }
 
     # -- native handle
@@ -509,6 +587,13 @@ class Simulation:
         if ratio.size:
             self._check(lib.fi_set_channel_scaling(h, ratio.size, abi.dptr(ratio), abi.dptr(thick)),
                         "fi_set_channel_scaling")
+        if inp["ocean_surface"] is not None:
+            z, A = (abi.as_f64(a) for a in inp["ocean_surface"])
+            self._check(lib.fi_set_ocean_surface_table(h, z.size, abi.dptr(z), abi.dptr(A)),
+                        "fi_set_ocean_surface_table")
+        if inp["bsl_history"] is not None:
+            t, z = (abi.as_f64(a) for a in inp["bsl_history"])
+            self._check(lib.fi_set_bsl_history(h, t.size, abi.dptr(t), abi.dptr(z)), "fi_set_bsl_history")
 
     def set_fft_schedule(self, L, radices):
         """Radix order of the length-L transforms (before init_problem)."""
@@ -539,6 +624,12 @@ class Simulation:
         if not self._initialized:
             self._check(self.lib.fi_init(self._handle), "fi_init")
             self._initialized = True
+
+    def sealevel_state(self):
+        """sim.now.z_bsl, bsl.A and the volume terms (fi_get_sealevel)."""
+        out = abi.FiSealevel()
+        self._check(self.lib.fi_get_sealevel(self._handle, C.byref(out)), "fi_get_sealevel")
+        return {k: getattr(out, k) for k, _ in abi.FiSealevel._fields_ if k != "pad"}
 
     def stats(self):
         st = abi.FiStats()

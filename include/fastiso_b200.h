@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FI_ABI_VERSION 1
+#define FI_ABI_VERSION 2
 
 /* ---- status codes (error(...) calls of the reference become these) ---- */
 enum {
@@ -90,7 +90,30 @@ typedef struct fi_config {
     int64_t max_steps;              /* step-attempt budget per run/step call (0 = unlimited) */
     int32_t form;                   /* FI_FORM_* */
     int32_t device;                 /* CUDA device ordinal the handle runs on */
+    /* RegionalSeaLevel beyond its surface (src/sealevel.jl:114-130,
+     * src/barystatic_sealevel.jl): the sea-level load, the barystatic sea level
+     * (BSL) and its update, the volume contributions.  Defaults: NoSealevelLoad,
+     * ConstantBSL, InternalBSLUpdate, Goelzer volume and density contributions, no
+     * adjustment contribution.  z_bsl above is the ReferenceBSL level ref.z. */
+    int32_t sealevel_load;          /* FI_SEALEVEL_LOAD_* */
+    int32_t bsl_mode;               /* FI_BSL_* */
+    int32_t bsl_update;             /* FI_BSL_UPDATE_* */
+    int32_t volume_contribution;    /* FI_CONTRIB_NONE or FI_CONTRIB_GOELZER */
+    int32_t density_contribution;   /* FI_CONTRIB_NONE or FI_CONTRIB_GOELZER */
+    int32_t adjustment_contribution;/* FI_CONTRIB_NONE or FI_CONTRIB_GOELZER */
+    double bsl_ref_A;               /* ReferenceBSL ocean area ref.A (m^2), A_OCEAN_PD = 3.625e14 */
 } fi_config;
+
+/* sealevel.load (src/loads.jl:1-27) */
+enum { FI_SEALEVEL_LOAD_NONE = 0, FI_SEALEVEL_LOAD_INTERACTIVE = 1 };
+/* sealevel.bsl (src/barystatic_sealevel.jl:100-200): ConstantBSL; ConstantOceanSurfaceBSL
+ * (z += dV / ref.A); PiecewiseConstantBSL (z += dV / A, then A = A_itp(z) from the table
+ * of fi_set_ocean_surface_table); ImposedBSL (z = z_itp(t) from fi_set_bsl_history). */
+enum { FI_BSL_CONSTANT = 0, FI_BSL_CONSTANT_OCEAN_SURFACE = 1, FI_BSL_PIECEWISE_CONSTANT = 2, FI_BSL_IMPOSED = 3 };
+/* sealevel.update_bsl: InternalBSLUpdate / ExternalBSLUpdate (delta_V only) */
+enum { FI_BSL_UPDATE_INTERNAL = 0, FI_BSL_UPDATE_EXTERNAL = 1 };
+/* volume / density / adjustment contributions (src/sealevel.jl:260-332) */
+enum { FI_CONTRIB_NONE = 0, FI_CONTRIB_GOELZER = 1 };
 
 /* Fields addressable by fi_set_field / fi_get_field.  All are nx*ny doubles. */
 enum {
@@ -117,8 +140,23 @@ enum {
     FI_FIELD_COLUMNANOM_LOAD = 19,    /* sim.now.columnanoms.load (get) */
     FI_FIELD_COLUMNANOM_FULL = 20,    /* sim.now.columnanoms.full (get) */
     FI_FIELD_H_AF = 21,               /* sim.now.H_af (get) */
-    FI_NUM_FIELDS = 22
+    FI_FIELD_MASKGROUNDED = 22,       /* sim.now.maskgrounded as 0/1 (get) */
+    FI_FIELD_MASKOCEAN = 23,          /* sim.now.maskocean as 0/1 (get) */
+    FI_FIELD_H_WATER = 24,            /* sim.now.H_water (get) */
+    FI_FIELD_COLUMNANOM_SEAWATER = 25,/* sim.now.columnanoms.seawater (get) */
+    FI_NUM_FIELDS = 26
 };
+
+/* Barystatic sea level and the volume terms of the last sparse update (sim.now.z_bsl,
+ * sim.sealevel.bsl.A, sim.now.V_af / V_den / V_pov / delta_V).  The FP32 form keeps the
+ * volumes only when they can act on the solution (an interactive sea-level load or a
+ * BSL other than ConstantBSL); otherwise `tracked` is 0 and they read 0. */
+typedef struct fi_sealevel {
+    double z_bsl, A_bsl;
+    double V_af, V_den, V_pov, delta_V;
+    int32_t tracked;
+    int32_t pad;
+} fi_sealevel;
 
 typedef struct fi_stats {
     double t;                 /* integrator time (yr) */
@@ -172,6 +210,15 @@ int fi_set_elastic_table(fi_handle* h, int32_t n, const double* rm, const double
  * FI_FIELD_PSEUDODIFF_SCALING field) R = 1, the one-layer case. */
 int fi_set_channel_scaling(fi_handle* h, int32_t n, const double* visc_ratio_mean,
                            const double* channel_thickness_mean);
+
+/* ReferenceBSL(z).A_itp (src/barystatic_sealevel.jl:36-42): the ocean surface area A(z)
+ * of PiecewiseConstantBSL, n strictly increasing levels z (m) with areas A (m^2) --
+ * the caller's copy of the table the reference downloads (unbiased so that A(0) is
+ * A_OCEAN_PD); linear inside, and z outside [z_0, z_{n-1}] is FI_ERR_FORCING_RANGE. */
+int fi_set_ocean_surface_table(fi_handle* h, int32_t n, const double* z, const double* A);
+
+/* ImposedBSL(t_vec, z_vec) (src/barystatic_sealevel.jl:172-181): z_bsl(t) linear in time. */
+int fi_set_bsl_history(fi_handle* h, int32_t n, const double* t, const double* z);
 
 /* No counterpart in the reference: tile shape of the FP32 kernels, between fi_create
  * and fi_init.  h_rows: rows per row task (row FFTs, stencils), B_cols: spectral
@@ -252,6 +299,9 @@ int fi_set_step_replay(fi_handle* h, int64_t n, const double* dts);
 
 /* Counters of the integrator and the RHS. */
 int fi_get_stats(fi_handle* h, fi_stats* st);
+
+/* sim.now.z_bsl, bsl.A and the volume terms of the last sparse update. */
+int fi_get_sealevel(fi_handle* h, fi_sealevel* out);
 
 /* Checkpoint: the full integrator + diagnostic state, behind a header that names the
  * library's checkpoint version, the compute form and the grid.  fi_checkpoint with

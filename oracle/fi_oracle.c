@@ -228,6 +228,11 @@ struct or_sim {
     double *u, *ue, *dudt, *H_ice, *H_af, *z_b, *dz_ss, *z_ss;
     double *c_ice, *c_sw, *c_sed, *c_litho, *c_mantle, *c_load, *c_full;
     int64_t count_sparse;
+    /* sea level beyond the surface (src/sealevel.jl:242-332, src/barystatic_sealevel.jl) */
+    double z_bsl, A_bsl, V_af, V_den, V_pov, delta_V;
+    double *H_water, *mask_gr, *mask_oc;
+    int n_osurf, n_bslh;
+    double *osurf_z, *osurf_A, *bslh_t, *bslh_z;
     /* work buffers */
     double *rhs, *bxx, *byy, *bx, *bxy, *Mxx, *Myy, *Mxy, *buf;
     cpx *fftrhs, *convbuf;
@@ -522,7 +527,7 @@ int or_create(const fi_config* cfg, or_sim** out) {
                          &s->z_ss_ref, &s->u, &s->ue, &s->dudt, &s->H_ice, &s->H_af, &s->z_b, &s->dz_ss,
                          &s->z_ss, &s->c_ice, &s->c_sw, &s->c_sed, &s->c_litho, &s->c_mantle, &s->c_load,
                          &s->c_full, &s->rhs, &s->bxx, &s->byy, &s->bx, &s->bxy, &s->Mxx, &s->Myy, &s->Mxy,
-                         &s->buf};
+                         &s->buf, &s->H_water, &s->mask_gr, &s->mask_oc};
     for (size_t k = 0; k < sizeof(fields) / sizeof(fields[0]); k++) *fields[k] = dalloc(n);
     for (size_t k = 0; k < n; k++) { s->R[k] = 1.0; s->mask[k] = 1.0; s->z_b_ref[k] = 1e6; }
     s->fftrhs = (cpx*)calloc(n, sizeof(cpx));
@@ -541,7 +546,8 @@ void or_destroy(or_sim* s) {
                       s->u, s->ue, s->dudt, s->H_ice, s->H_af, s->z_b, s->dz_ss, s->z_ss, s->c_ice, s->c_sw,
                       s->c_sed, s->c_litho, s->c_mantle, s->c_load, s->c_full, s->rhs, s->bxx, s->byy, s->bx,
                       s->bxy, s->Mxx, s->Myy, s->Mxy, s->buf, s->cropped, s->rm, s->GE, s->t_ice, s->H_tab,
-                      s->ch_ratio, s->ch_thick, s->tout_copy};
+                      s->ch_ratio, s->ch_thick, s->tout_copy, s->H_water, s->mask_gr, s->mask_oc,
+                      s->osurf_z, s->osurf_A, s->bslh_t, s->bslh_z};
     for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); k++) free(ptrs[k]);
     free(s->fftrhs); free(s->convbuf); free(s->Ge_hat); free(s->Gg_hat);
     fft_plan_free(&s->fx); fft_plan_free(&s->fy); fft_plan_free(&s->fMx); fft_plan_free(&s->fMy);
@@ -577,6 +583,10 @@ static double* field_ptr(or_sim* s, int32_t f, int for_set) {
         case FI_FIELD_COLUMNANOM_LOAD: return s->c_load;
         case FI_FIELD_COLUMNANOM_FULL: return s->c_full;
         case FI_FIELD_H_AF: return s->H_af;
+        case FI_FIELD_MASKGROUNDED: return for_set ? NULL : s->mask_gr;
+        case FI_FIELD_MASKOCEAN: return for_set ? NULL : s->mask_oc;
+        case FI_FIELD_H_WATER: return for_set ? NULL : s->H_water;
+        case FI_FIELD_COLUMNANOM_SEAWATER: return for_set ? NULL : s->c_sw;
         default: return NULL;
     }
 }
@@ -632,6 +642,117 @@ int or_set_channel_scaling(or_sim* s, int32_t n, const double* ratio, const doub
     s->ch_thick = dalloc(n);
     if (n) { memcpy(s->ch_ratio, ratio, sizeof(double) * n); memcpy(s->ch_thick, thick, sizeof(double) * n); }
     return FI_OK;
+}
+
+static int copy_table_(or_sim* s, int32_t n, const double* x, const double* y, int* n_out, double** xo, double** yo) {
+    if (n < 2 || !x || !y) return set_err(s, FI_ERR_ARG, "a table needs >= 2 points");
+    for (int k = 1; k < n; k++)
+        if (!(x[k] > x[k - 1])) return set_err(s, FI_ERR_ARG, "table abscissae must increase");
+    free(*xo); free(*yo);
+    *xo = dalloc(n); *yo = dalloc(n);
+    memcpy(*xo, x, sizeof(double) * n);
+    memcpy(*yo, y, sizeof(double) * n);
+    *n_out = n;
+    return FI_OK;
+}
+
+int or_set_ocean_surface_table(or_sim* s, int32_t n, const double* z, const double* A) {
+    if (!s) return FI_ERR_ARG;
+    return copy_table_(s, n, z, A, &s->n_osurf, &s->osurf_z, &s->osurf_A);
+}
+
+int or_set_bsl_history(or_sim* s, int32_t n, const double* t, const double* z) {
+    if (!s) return FI_ERR_ARG;
+    return copy_table_(s, n, t, z, &s->n_bslh, &s->bslh_t, &s->bslh_z);
+}
+
+/* interpolate(x, ::TimeInterpolation0D) with flat_bc = false (src/interpolations.jl:20-40):
+ * linear inside the table, an error outside */
+static int interp0d_(const double* xs, const double* ys, int n, double x, double* y) {
+    if (n < 2 || x < xs[0] || x > xs[n - 1]) return FI_ERR_FORCING_RANGE;
+    int k = 0;
+    while (k < n - 2 && xs[k + 1] < x) k++;
+    const double w = (x - xs[k]) / (xs[k + 1] - xs[k]);
+    *y = ys[k] + w * (ys[k + 1] - ys[k]);
+    return FI_OK;
+}
+
+int or_get_sealevel(or_sim* s, fi_sealevel* out) {
+    if (!s || !out) return FI_ERR_ARG;
+    memset(out, 0, sizeof(*out));
+    out->z_bsl = s->z_bsl; out->A_bsl = s->A_bsl;
+    out->V_af = s->V_af; out->V_den = s->V_den; out->V_pov = s->V_pov; out->delta_V = s->delta_V;
+    out->tracked = 1;
+    return FI_OK;
+}
+
+/* update_V_af!, update_V_den!, update_V_pov! (src/sealevel.jl:275-332) on the current
+ * H_af, H_ice, z_ss and z_b; returns the total volume */
+static double update_volumes_(or_sim* s) {
+    const fi_config* c = &s->cfg;
+    const size_t n = (size_t)s->nx * s->ny;
+    double saf = 0.0, sden = 0.0, spov = 0.0;
+    for (size_t k = 0; k < n; k++) {
+        saf += s->H_af[k] * s->A;
+        sden += s->H_ice[k] * s->A;
+        const double w = s->z_ss[k] - s->z_b[k];
+        spov += (w > 0 ? w : 0.0) * s->A;
+    }
+    s->V_af = c->volume_contribution == FI_CONTRIB_GOELZER ? saf * c->rho_ice / c->rho_seawater : 0.0;
+    s->V_den = c->density_contribution == FI_CONTRIB_GOELZER
+                   ? sden * (c->rho_ice / c->rho_water - c->rho_ice / c->rho_seawater) : 0.0;
+    s->V_pov = c->adjustment_contribution == FI_CONTRIB_GOELZER ? spov : 0.0;
+    return s->V_af + s->V_den + s->V_pov;
+}
+
+/* internal_update_bsl! (src/sealevel.jl:242-262) with update_bsl! of each BSL
+ * (src/barystatic_sealevel.jl:215-235) */
+static int internal_update_bsl_(or_sim* s, double t) {
+    const fi_config* c = &s->cfg;
+    const double Vold = s->V_af + s->V_den + s->V_pov;
+    s->delta_V = update_volumes_(s) - Vold;
+    if (c->bsl_update != FI_BSL_UPDATE_INTERNAL) return FI_OK;
+    const double dV = -s->delta_V;
+    switch (c->bsl_mode) {
+        case FI_BSL_CONSTANT: s->z_bsl = c->z_bsl; break;
+        case FI_BSL_CONSTANT_OCEAN_SURFACE: s->A_bsl = c->bsl_ref_A; s->z_bsl += dV / s->A_bsl; break;
+        case FI_BSL_PIECEWISE_CONSTANT: {
+            s->z_bsl += dV / s->A_bsl;
+            double A;
+            if (interp0d_(s->osurf_z, s->osurf_A, s->n_osurf, s->z_bsl, &A))
+                return set_err(s, FI_ERR_FORCING_RANGE, "BSL %g outside the ocean-surface table", s->z_bsl);
+            s->A_bsl = A;
+            break;
+        }
+        case FI_BSL_IMPOSED: {
+            double z;
+            if (interp0d_(s->bslh_t, s->bslh_z, s->n_bslh, t, &z))
+                return set_err(s, FI_ERR_FORCING_RANGE, "t = %g outside the imposed BSL history", t);
+            s->z_bsl = z;
+            break;
+        }
+        default: return set_err(s, FI_ERR_ARG, "unknown BSL mode %d", c->bsl_mode);
+    }
+    return FI_OK;
+}
+
+/* update_maskgrounded!, update_maskocean!, watercolumn! and columnanom_water!
+ * (src/topography.jl:1-28, src/loads.jl:56-85) on the current fields */
+static void masks_water_(or_sim* s) {
+    const fi_config* c = &s->cfg;
+    const size_t n = (size_t)s->nx * s->ny;
+    const int interactive = c->sealevel_load == FI_SEALEVEL_LOAD_INTERACTIVE;
+    for (size_t k = 0; k < n; k++) {
+        const int gr = s->H_af[k] > 0;
+        const double w = s->z_ss[k] - s->z_b[k];
+        const int oc = (w > 0) && !gr;
+        s->mask_gr[k] = gr;
+        s->mask_oc[k] = oc;
+        const double wc = w > 0 ? w : 0.0;
+        const double H = s->H_ice[k];
+        s->H_water[k] = (H <= 1 ? wc : 0.0) + ((!gr && H > 1) ? wc - H * (c->rho_ice / c->rho_seawater) : 0.0);
+        s->c_sw[k] = interactive ? c->rho_seawater * (s->z_ss[k] - s->z_ss_ref[k]) * oc * s->mask[k] : 0.0;
+    }
 }
 
 /* interpolate!(X_out, t, ::TimeInterpolation2D), src/interpolations.jl:51-74 */
@@ -712,7 +833,11 @@ static int rhs_impl(or_sim* s, double t, double* u, double* dudt) {
         }
         /* columnanom_litho! */
         for (size_t k = 0; k < n; k++) s->c_litho[k] = c->rho_litho * (s->ue[k] - s->ue_ref[k]);
-        /* internal_update_bsl!: ConstantBSL keeps z_bsl = ref.z */
+        /* internal_update_bsl!, src/sealevel.jl:242-262 */
+        {
+            int rc = internal_update_bsl_(s, t);
+            if (rc) return rc;
+        }
         /* update_dz_ss!(sim, surface), src/sealevel.jl:173-201 */
         if (c->sea_surface == FI_SEA_SURFACE_LATERALLY_VARIABLE) {
             if (c->lithosphere_column == FI_COLUMN_COMPRESSIBLE)
@@ -721,13 +846,13 @@ static int rhs_impl(or_sim* s, double t, double* u, double* dudt) {
                 for (size_t k = 0; k < n; k++) s->buf[k] = s->A * s->c_full[k];
             samesize_conv_ext(s, s->dz_ss, s->buf, s->Gg_hat, c->bc_sea_surface_border);
         }
-        /* update_z_ss!, update_Haf!, masks, columnanom_water!(NoSealevelLoad), columnanom_ice! */
+        /* update_z_ss!, update_Haf!, masks, columnanom_water!, columnanom_ice! */
         for (size_t k = 0; k < n; k++) {
-            s->z_ss[k] = s->z_ss_ref[k] + s->dz_ss[k] + c->z_bsl;
+            s->z_ss[k] = s->z_ss_ref[k] + s->dz_ss[k] + s->z_bsl;
             s->H_af[k] = haf_(s, s->H_ice[k], s->z_b[k], s->z_ss[k]);
-            s->c_sw[k] = 0.0;
-            s->c_ice[k] = c->rho_ice * (s->H_af[k] - s->H_af_ref[k]);
         }
+        masks_water_(s);
+        for (size_t k = 0; k < n; k++) s->c_ice[k] = c->rho_ice * (s->H_af[k] - s->H_af_ref[k]);
         s->count_sparse += 1;
     }
     /* columnanom_load!, columnanom_full!, src/loads.jl:96-106 */
@@ -822,6 +947,12 @@ static int setup_(or_sim* s) {
         s->c_ice[k] = s->c_sw[k] = s->c_sed[k] = s->c_litho[k] = s->c_mantle[k] = s->c_load[k] = s->c_full[k] = 0.0;
         s->dudt[k] = 0.0;
     }
+    /* ReferenceState masks and water column; CurrentState copies them */
+    s->z_bsl = c->z_bsl;
+    s->A_bsl = c->bsl_ref_A > 0 ? c->bsl_ref_A : 3.625e14;
+    masks_water_(s);
+    for (size_t k = 0; k < n; k++) s->c_sw[k] = 0.0; /* ColumnAnomalies start at zero */
+    s->V_af = s->V_den = s->V_pov = s->delta_V = 0.0;
     s->count_sparse = 0;
     return FI_OK;
 }
@@ -831,9 +962,18 @@ int or_init(or_sim* s) {
     /* u defaults to copy(u_ref) unless set explicitly */
     const size_t n = (size_t)s->nx * s->ny;
     if (!s->u_set) memcpy(s->u, s->u_ref, n * sizeof(double));
+    if (s->cfg.sealevel_load == FI_SEALEVEL_LOAD_INTERACTIVE) {
+        double active = 0.0;
+        for (size_t k = 0; k < n; k++) active += s->mask[k] != 0.0;
+        if (active > 0.6 * (double)n)
+            return set_err(s, FI_ERR_ARG, "Mask defining regions of active load must not cover more than 60%% "
+                                          "of the cells when using an interactive sea level.");
+    }
     int rc = setup_(s);
     if (rc) return rc;
-    /* init_problem!: the first update_diagnostics! at t0 (forces the sparse update) */
+    /* init_problem!: the volumes of the initial state, then the first
+     * update_diagnostics! at t0 (forces the sparse update), src/simulation.jl:305-312 */
+    update_volumes_(s);
     double* du = dalloc(n);
     rc = rhs_impl(s, s->cfg.t0, s->u, du);
     free(du);
@@ -1126,7 +1266,13 @@ static void record_(void* ctx, int k, double t) {
     if (s->out_dz_ss) memcpy(s->out_dz_ss + (size_t)k * n, s->dz_ss, n * sizeof(double));
 }
 
+static int start_integrator_at_(or_sim* s, double t_start, int32_t n_tstops, const double* tstops);
+
 static int start_integrator_(or_sim* s, int32_t n_tstops, const double* tstops) {
+    return start_integrator_at_(s, s->cfg.t0, n_tstops, tstops);
+}
+
+static int start_integrator_at_(or_sim* s, double t_start, int32_t n_tstops, const double* tstops) {
     or_integ* I = &s->I;
     integ_alloc(I, s->nx * s->ny);
     I->f = rhs_cb;
@@ -1137,7 +1283,7 @@ static int start_integrator_(or_sim* s, int32_t n_tstops, const double* tstops) 
     I->record = record_;
     I->kout = 0;
     /* run! constructs the ODEProblem on sim.now.u after init_problem! */
-    int rc = integ_start(I, s->u, s->cfg.t0, s->cfg.t1);
+    int rc = integ_start(I, s->u, t_start, s->cfg.t1);
     if (rc) return rc;
     for (int k = 0; k < n_tstops; k++) tstop_add(I, tstops[k]);
     return FI_OK;
@@ -1172,6 +1318,43 @@ int or_init_integrator(or_sim* s, int32_t n_tstops, const double* tstops) {
     if (n_tstops) memcpy(s->tout_copy, tstops, sizeof(double) * n_tstops);
     s->out_t = NULL; s->out_u = s->out_ue = s->out_dudt = s->out_dz_ss = NULL;
     int rc = start_integrator_(s, n_tstops, tstops);
+    s->I.nout = n_tstops;
+    s->I.tout = s->tout_copy;
+    s->I.kout = 0;
+    return rc;
+}
+
+/* Resume at time t from a state computed elsewhere (u, ue, dz_ss and the sparse-update
+ * count at t): the diagnostics of the last update_diagnostics! call at (t, u) are
+ * rebuilt with the sparse gate held shut, then the integrator starts at t as
+ * init_integrator does at t0 (initial dt heuristic, tstops with output callbacks).
+ * Test infrastructure: times the oracle over a window that starts late in a run. */
+int or_resume(or_sim* s, double t, int64_t count_sparse, const double* u, const double* ue, const double* dz_ss,
+              int32_t n_tstops, const double* tstops) {
+    if (!s || !u || !ue || !dz_ss || n_tstops < 0 || (n_tstops > 0 && !tstops)) return FI_ERR_ARG;
+    if (!s->initialized) return set_err(s, FI_ERR_STATE, "or_init not called");
+    const fi_config* c = &s->cfg;
+    const size_t n = (size_t)s->nx * s->ny;
+    memcpy(s->ue, ue, n * sizeof(double));
+    memcpy(s->dz_ss, dz_ss, n * sizeof(double));
+    for (size_t k = 0; k < n; k++) {
+        s->c_litho[k] = c->rho_litho * (s->ue[k] - s->ue_ref[k]);
+        s->z_ss[k] = s->z_ss_ref[k] + s->dz_ss[k] + c->z_bsl;
+    }
+    double* uu = dalloc(n);
+    double* du = dalloc(n);
+    memcpy(uu, u, n * sizeof(double));
+    s->count_sparse = INT64_MAX; /* gate shut for the rebuild */
+    int rc = rhs_impl(s, t, uu, du);
+    s->count_sparse = count_sparse;
+    free(uu);
+    free(du);
+    if (rc) return rc;
+    free(s->tout_copy);
+    s->tout_copy = dalloc(n_tstops);
+    if (n_tstops) memcpy(s->tout_copy, tstops, sizeof(double) * n_tstops);
+    s->out_t = NULL; s->out_u = s->out_ue = s->out_dudt = s->out_dz_ss = NULL;
+    rc = start_integrator_at_(s, t, n_tstops, tstops);
     s->I.nout = n_tstops;
     s->I.tout = s->tout_copy;
     s->I.kout = 0;

@@ -30,10 +30,15 @@ int or_run(or_sim* s, int32_t n_out, const double* t_out, double* out_t,
            double* out_u, double* out_ue, double* out_dudt, double* out_dz_ss);
 int or_init_integrator(or_sim* s, int32_t n_tstops, const double* tstops);
 int or_step(or_sim* s, double dt);
+int or_resume(or_sim* s, double t, int64_t count_sparse, const double* u, const double* ue, const double* dz_ss,
+              int32_t n_tstops, const double* tstops);
 int or_record_steps(or_sim* s, int64_t cap);
 int or_get_step_record(or_sim* s, double* dts, int64_t cap, int64_t* n);
 int or_set_step_replay(or_sim* s, int64_t n, const double* dts);
 int or_get_stats(or_sim* s, fi_stats* st);
+int or_get_sealevel(or_sim* s, fi_sealevel* out);
+int or_set_ocean_surface_table(or_sim* s, int32_t n, const double* z, const double* A);
+int or_set_bsl_history(or_sim* s, int32_t n, const double* t, const double* z);
 const char* or_last_error(const or_sim* s);
 void or_destroy(or_sim* s);
 void or_set_threads(int32_t n);

@@ -46,6 +46,10 @@ def lib():
         "or_step": (C.c_int, [C.c_void_p, C.c_double]),
         "or_get_stats": (C.c_int, [C.c_void_p, C.POINTER(FiStats)]),
         "or_record_steps": (C.c_int, [C.c_void_p, C.c_int64]),
+        "or_get_sealevel": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "or_set_ocean_surface_table": (C.c_int, [C.c_void_p, C.c_int32, dp, dp]),
+        "or_set_bsl_history": (C.c_int, [C.c_void_p, C.c_int32, dp, dp]),
+        "or_resume": (C.c_int, [C.c_void_p, C.c_double, C.c_int64, dp, dp, dp, C.c_int32, dp]),
         "or_get_step_record": (C.c_int, [C.c_void_p, dp, C.c_int64, C.POINTER(C.c_int64)]),
         "or_set_step_replay": (C.c_int, [C.c_void_p, C.c_int64, dp]),
         "or_last_error": (C.c_char_p, [C.c_void_p]),
@@ -144,6 +148,31 @@ class OracleSim:
     def step(self, dt):
         self._check(lib().or_step(self.h, float(dt)), "step")
 
+    def sealevel(self):
+        from fastiso_b200.abi import FiSealevel
+
+        out = FiSealevel()
+        self._check(lib().or_get_sealevel(self.h, C.byref(out)), "get_sealevel")
+        return {k: getattr(out, k) for k, _ in FiSealevel._fields_ if k != "pad"}
+
+    def set_ocean_surface_table(self, z, A):
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        self._check(lib().or_set_ocean_surface_table(self.h, z.size, _p(z), _p(A)), "set_ocean_surface_table")
+
+    def set_bsl_history(self, t, z):
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        z = np.ascontiguousarray(z, dtype=np.float64)
+        self._check(lib().or_set_bsl_history(self.h, t.size, _p(t), _p(z)), "set_bsl_history")
+
+    def resume(self, t, count_sparse, u, ue, dz_ss, tstops=()):
+        """Start the integrator at t from a state computed elsewhere (flat x-fastest
+        u, ue, dz_ss and the sparse-update count at t)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (u, ue, dz_ss)]
+        ts = np.ascontiguousarray(tstops, dtype=np.float64)
+        self._check(lib().or_resume(self.h, float(t), int(count_sparse), *[_p(a) for a in arrs], ts.size,
+                                    _p(ts) if ts.size else None), "resume")
+
     def record_steps(self, cap):
         self._check(lib().or_record_steps(self.h, int(cap)), "record_steps")
 
@@ -237,4 +266,8 @@ def oracle_for(sim):
     ratio, thick = inp["channels"]
     if ratio.size:
         ref.set_channel_scaling(ratio, thick)
+    if inp.get("ocean_surface") is not None:
+        ref.set_ocean_surface_table(*inp["ocean_surface"])
+    if inp.get("bsl_history") is not None:
+        ref.set_bsl_history(*inp["bsl_history"])
     return ref

@@ -100,3 +100,37 @@ def oracle_outputs(ref, t_outs, fields=("u", "dudt", "dz_ss"), record=0, replay=
         for f in fields:
             out[f].append(ref.get_field(ORACLE_FIELD_IDS[f]))
     return out, (ref.step_record() if record else None)
+
+
+def sealevel_sim(form, bsl=None, interactive=True, nx=40, ny=36, t_end=400.0, seed=21, adjustment=False):
+    """A coastal case for the sea-level rows: bedrock from +600 m at the centre to
+    -1400 m at the edges (an ocean all around), a disc of ice thick enough to ground
+    on the shelf, active-load mask on the inner 40 % of the width (under the 60 % limit
+    of interactive sea levels) reaching into the ocean beyond 0.3 of the width, elastic,
+    viscous and sea-surface convolutions on."""
+    W_ = 0.8e6
+    domain = F.RegionalDomain(W_, W_ * ny / nx, nx, ny)
+    rng = np.random.default_rng(seed)
+    log10eta = 21 + 0.3 * np.exp(-domain.R**2 / (2 * (W_ / 3) ** 2)) + 0.05 * rng.standard_normal((nx, ny))
+    T = 100e3 + 20e3 * rng.random((nx, ny))
+    mask = domain.R < 0.45 * W_
+    se = F.SolidEarth(domain, layer_boundaries=T.reshape(nx, ny, 1),
+                      layer_viscosities=(10**log10eta).reshape(nx, ny, 1), maskactive=mask)
+    z_b_ref = 600.0 - 2000.0 * domain.R / W_
+    H1 = 2.5e3 * (domain.R < 0.25 * W_)
+    it = F.TimeInterpolatedIceThickness([0.0, 1.0, 200.0, max(t_end, 400.0)], [domain.zeros(), H1, 0.4 * H1, 0.2 * H1],
+                                        domain)
+    bcs = F.BoundaryConditions(domain, ice_thickness=it)
+    sl = F.RegionalSeaLevel(surface=F.LaterallyVariableSeaSurface(),
+                            load=F.InteractiveSealevelLoad() if interactive else F.NoSealevelLoad(),
+                            bsl=bsl if bsl is not None else F.ConstantBSL(),
+                            adjustment_contribution=(F.GoelzerAdjustmentContribution() if adjustment
+                                                     else F.NoAdjustmentContribution()))
+    return F.Simulation(domain, bcs, sl, se, (0.0, t_end), z_b_ref=z_b_ref, form=form)
+
+
+def ocean_surface_table():
+    """A synthetic ocean-area table A(z) for PiecewiseConstantBSL (the reference downloads
+    one): +-200 m around the present level, A(0) = A_OCEAN_PD, 3 % area change per 100 m."""
+    z = np.linspace(-200.0, 200.0, 41)
+    return z, abi.A_OCEAN_PD * (1.0 + 3e-4 * z)

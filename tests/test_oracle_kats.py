@@ -159,3 +159,29 @@ def test_oracle_replay_reproduces_its_run():
         np.testing.assert_array_equal(b.get_field(8), u)
     st_b = b.stats()
     assert (st_b["naccept"], st_b["nreject"], st_b["nsparse"]) == (st_a["naccept"], st_a["nreject"], st_a["nsparse"])
+
+
+def test_oracle_resume_continues_the_run():
+    """or_resume at t from a state taken at t continues the same solution: it differs
+    from the uninterrupted run only by the restarted step sequence (new initial dt),
+    i.e. by the integrator's own error."""
+    import fastiso_b200.workloads as W
+
+    def fresh():
+        sim = W.config2(form="fp64", N=32, t_end=600.0, out_every=600.0, n_snap=2)
+        r = O.oracle_for(sim)
+        r.init()
+        return r
+
+    a = fresh()
+    a.init_integrator([300.0, 600.0])
+    a.step(300.0)
+    st = a.stats()
+    state = [a.get_field(i) for i in (8, 9, 11)]  # u, ue, dz_ss
+    b = fresh()
+    b.resume(st["t"], st["nsparse"], *state, tstops=[600.0])
+    assert b.stats()["t"] == 300.0
+    a.step(300.0)
+    b.step(300.0)
+    assert rel_l2(b.get_field(8), a.get_field(8)) < 2e-3
+    assert b.stats()["nsparse"] >= st["nsparse"] + 29

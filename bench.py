@@ -328,6 +328,30 @@ def config5_bench(dev):
             "clocks": clk.summary()}
 
 
+def output_bench(dev, kyr=2.0, every=100.0):
+    """run! on the N = 350 workload over the first `kyr` kyr with NativeOutput every
+    `every` yr (u, ue, dudt, dz_ss: 4 x 1 MB per output through the asynchronous
+    staging / copy-stream pipeline) against the same run with a single output at the
+    end; wall clock of the whole fi_run call, so the host side of the outputs counts."""
+    res = {}
+    for name, outs in (("every", list(np.arange(every, kyr * 1e3 + 1, every))), ("end_only", [kyr * 1e3])):
+        sim = W.config2(form="fp32", N=N350, t_end=kyr * 1e3)
+        sim.cfg.device = dev
+        sim.cfg.max_steps = 20_000_000
+        sim.nout.t = [float(t) for t in outs]
+        sim.init_problem()
+        t0 = time.perf_counter()
+        F.run(sim)
+        el = time.perf_counter() - t0
+        assert all(np.isfinite(a).all() for a in sim.nout.out["u"])
+        res[name] = {"kyr_per_s": kyr / el, "outputs": len(outs), "wall_s": el}
+        sim.close()
+    res["ratio"] = res["every"]["kyr_per_s"] / res["end_only"]["kyr_per_s"]
+    res["note"] = (f"fi_run over 0..{kyr:g} kyr; outputs of u, ue, dudt, dz_ss every {every:g} yr vs one at the end "
+                   "(each output also re-evaluates the FSAL derivative, as the reference's output callback does)")
+    return res
+
+
 def fno_flops_per_sample(S=128, C=32, KX=16, KY=32, PW=128, nin=6, layers=4):
     """Algorithmic FLOPs of one forward pass of the surrogate per sample (the GEMMs as
     contracted, without padding): lift, per layer the DFT along x and y, the mode mixing,
@@ -603,6 +627,7 @@ def run_gpu(args, rank, world, dev):
     # ---- the surrogate network and the N = 1024 case (outside the timed region) ----
     surrogate = fno_bench(dev, 20, max(3, args.warmup))
     config5 = config5_bench(dev)
+    outputs = output_bench(dev)
     # ---- CPU baseline: the oracle resumed at the window start --------------------
     cores = os.cpu_count() or 1
     cpu_all, yrs_all = oracle_resumed(p64["start"], cores, 12.0)
@@ -631,6 +656,7 @@ def run_gpu(args, rank, world, dev):
         "ensemble": ens,
         "surrogate": surrogate,
         "config5": config5,
+        "output_pipeline": outputs,
         "e2e": {"value": e2e_val, "unit": "kyr/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                 "path": "per step: fi_set_field(u) from pinned host memory -> fi_step(1 kyr, the resident "
                         "time-interpolated ice history) -> fi_get_field(u) into pinned host memory; wall clock"},
@@ -665,6 +691,8 @@ def main():
                     help="N=1024: 5 yr warm-up launch, then one 0.2-yr launch of k_persist (ncu capture target)")
     ap.add_argument("--config5", action="store_true",
                     help="only the N=1024 high-resolution case (short window, roofline, rel-L2 vs FP64)")
+    ap.add_argument("--outputs", action="store_true",
+                    help="only the output-pipeline leg (run! with outputs every 100 yr vs one output)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -696,6 +724,9 @@ def main():
         return
     if args.config5:
         print(json.dumps({"config5": config5_bench(local)}), flush=True)
+        return
+    if args.outputs:
+        print(json.dumps({"output_pipeline": output_bench(local)}), flush=True)
         return
     if args.profile_config5:
         sim = W.config5(form="fp32")

@@ -20,3 +20,4 @@ from .model import (  # noqa: F401
     GoelzerVolumeContribution, ImposedBSL, InteractiveSealevelLoad, InternalBSLUpdate, NoAdjustmentContribution,
     NoDensityContribution, NoVolumeContribution, PiecewiseConstantBSL, ReferenceBSL,
 )
+from .model import LaterallyConstantLithosphere, RelaxedMantle, RigidMantle  # noqa: F401

@@ -50,6 +50,12 @@ FI_CONTRIB_NONE = 0
 FI_CONTRIB_GOELZER = 1
 #: A_OCEAN_PD, present-day ocean surface (m^2), src/barystatic_sealevel.jl:1
 A_OCEAN_PD = 3.625e14
+FI_LITHO_LATERALLY_CONSTANT = 2
+FI_MANTLE_MAXWELL = 0
+FI_MANTLE_RELAXED = 1
+FI_MANTLE_RIGID = 2
+FI_ALG_BS3 = 0
+FI_ALG_EULER = 1
 FI_EXEC_PERSIST = 0
 FI_EXEC_GRAPH = 1
 FI_EXEC_LOOP = 2
@@ -87,6 +93,8 @@ FIELDS = {
     "maskocean": 23,
     "H_water": 24,
     "columnanom_seawater": 25,
+    "tau": 26,
+    "u_eq": 27,
 }
 
 #: Float64(1f-5): the reference passes reltol as a Float32 literal (src/simulation.jl:13)
@@ -137,6 +145,9 @@ class FiConfig(C.Structure):
         ("density_contribution", C.c_int32),
         ("adjustment_contribution", C.c_int32),
         ("bsl_ref_A", C.c_double),
+        ("mantle", C.c_int32),
+        ("alg", C.c_int32),
+        ("dt_min", C.c_double),
     ]
 
 
@@ -214,6 +225,9 @@ def default_config(nx: int, ny: int, Wx: float, Wy: float) -> FiConfig:
     c.density_contribution = FI_CONTRIB_GOELZER
     c.adjustment_contribution = FI_CONTRIB_NONE
     c.bsl_ref_A = A_OCEAN_PD
+    c.mantle = FI_MANTLE_MAXWELL
+    c.alg = FI_ALG_BS3
+    c.dt_min = 0.0
     return c
 
 

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <complex>
 #include <map>
 #include <string>
 #include <vector>
@@ -48,6 +49,8 @@ struct PlainBufs {
     double2 *fftrhs, *P;
     double *D, *eta, *mask, *u_ref, *ue_ref, *z_b_ref, *z_ss_ref, *H_af_ref, *H_tab;
     double *s_sw, *mgr, *moc, *hwater;  // seawater anomaly, masks, water column
+    double *tau, *u_eq;                 // ELRA relaxation time and equilibrium displacement
+    double2 *Gv_hat, *fftU;             // ELRA kernel spectrum; spectrum of u (laterally-constant Maxwell)
     double2 *Ge_hat, *Gg_hat;
 };
 
@@ -67,7 +70,7 @@ struct fi_handle {
     FftPlan* d_plans = nullptr;
     int plan_x, plan_y, plan_Mx, plan_My;
     // host-side inputs
-    std::vector<double> D, eta, R, mask, u_ref, ue_ref, dz_ss_ref, z_b_ref, u_init;
+    std::vector<double> D, eta, R, mask, u_ref, ue_ref, dz_ss_ref, z_b_ref, u_init, tau;
     bool R_given = false, u_set = false;
     std::vector<double> ice_t, ice_H;
     std::vector<double> rm, GE;
@@ -116,6 +119,17 @@ struct fi_handle {
     size_t smem_cap = 0;
     double last_rhs_t = 0.0;
     long long nf_plain = 0;
+    // asynchronous output pipeline of fi_run: two staging slots (device FP64 copies of
+    // u, ue, dudt, dz_ss), read back on a copy stream into pinned host slots
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t ev_staged[2] = {nullptr, nullptr}, ev_copied[2] = {nullptr, nullptr};
+    double* d_out_slot[2] = {nullptr, nullptr};
+    double* h_out_slot[2] = {nullptr, nullptr};
+    struct PendingOut {
+        bool busy = false;
+        int k = 0;
+        double* dst[4] = {nullptr, nullptr, nullptr, nullptr};
+    } pend[2];
     // sea level: tables of PiecewiseConstantBSL (z -> A) and ImposedBSL (t -> z)
     std::vector<double> osurf_z, osurf_A, bslh_t, bslh_z;
     // step-sequence record / replay buffers (FP32 form: device, plain form: host)
@@ -329,6 +343,7 @@ int fi_create(const fi_config* cfg, fi_handle** out) {
     h->dz_ss_ref.assign(n, 0.0);
     h->z_b_ref.assign(n, 1e6);
     h->u_init.assign(n, 0.0);
+    h->tau.assign(n, 855.0);  // DEFAULT_MANTLE_TAU, src/solidearth.jl:121
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
         return FI_ERR_CUDA;
@@ -361,6 +376,16 @@ void fi_destroy(fi_handle* h) {
     for (void* p : h->allocs) cudaFree(p);
     if (h->d_rec) cudaFree(h->d_rec);
     if (h->d_replay) cudaFree(h->d_replay);
+    for (int q = 0; q < 2; q++) {
+        if (h->ev_staged[q]) cudaEventDestroy(h->ev_staged[q]);
+        if (h->ev_copied[q]) cudaEventDestroy(h->ev_copied[q]);
+        if (h->d_out_slot[q]) cudaFree(h->d_out_slot[q]);
+        if (h->h_out_slot[q]) cudaFreeHost(h->h_out_slot[q]);
+    }
+    if (h->cstream) {
+        cudaStreamSynchronize(h->cstream);
+        cudaStreamDestroy(h->cstream);
+    }
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -496,12 +521,13 @@ static int create_buffers(fi_handle* h) {
                            &p.now_u, &p.ue, &p.dz, &p.H, &p.H_af, &p.z_b, &p.z_ss, &p.s_i, &p.s_l, &p.s_m,
                            &p.s_load, &p.s_full, &p.dudt, &p.rhs, &p.bxx, &p.byy, &p.bx, &p.bxy, &p.Mxx,
                            &p.Myy, &p.Mxy, &p.buf, &p.D, &p.eta, &p.mask, &p.u_ref, &p.ue_ref, &p.z_b_ref,
-                           &p.z_ss_ref, &p.H_af_ref, &p.s_sw, &p.mgr, &p.moc, &p.hwater};
+                           &p.z_ss_ref, &p.H_af_ref, &p.s_sw, &p.mgr, &p.moc, &p.hwater, &p.tau, &p.u_eq};
         for (double** b : bufs) RET(dalloc(h, b, n));
         RET(dalloc(h, &p.cropped, (size_t)(2 * h->nx - 1) * (2 * h->ny - 1)));
         RET(dalloc(h, &p.off, 4));
         RET(dalloc(h, &p.partial, 3 * (size_t)h->red_blocks));
         RET(dalloc(h, &p.fftrhs, n));
+        RET(dalloc(h, &p.fftU, n));
         RET(dalloc(h, &p.P, M));
         RET(dalloc(h, &p.Ge_hat, M));
         RET(dalloc(h, &p.Gg_hat, M));
@@ -636,6 +662,11 @@ extern "C" int fi_set_field(fi_handle* h, int32_t field, const double* host, siz
         case FI_FIELD_UE_REF: h->ue_ref = v; return FI_OK;
         case FI_FIELD_DZ_SS_REF: h->dz_ss_ref = v; return FI_OK;
         case FI_FIELD_Z_B_REF: h->z_b_ref = v; return FI_OK;
+        case FI_FIELD_TAU:
+            for (double x : v)
+                if (!(x > 0)) return set_err(h, FI_ERR_ARG, "tau must be positive");
+            h->tau = v;
+            return FI_OK;
         case FI_FIELD_U: h->u_init = v; h->u_set = true; return FI_OK;
         case FI_FIELD_H_ICE:
             if (h->cfg.ice_mode != FI_ICE_EXTERNAL)
@@ -755,6 +786,42 @@ static int build_kernel_spectrum(fi_handle* h, const double* G, float2* half32, 
     return FI_OK;
 }
 
+// K_0(z) of a complex argument with Re z > 0: K_0(z) = int_0^inf exp(-z cosh t) dt
+// (Abramowitz & Stegun 9.6.24), trapezoidal rule with step 1/20 -- the integrand is
+// entire and decays doubly exponentially, so the rule converges geometrically (about
+// 1e-15 relative on the ray arg z = pi/4 that the Kelvin function uses).
+static std::complex<double> bessel_k0(std::complex<double> z) {
+    const double step = 0.05;
+    std::complex<double> acc = 0.5 * std::exp(-z);
+    for (int k = 1; k < 4000; k++) {
+        const std::complex<double> v = std::exp(-z * std::cosh(k * step));
+        acc += v;
+        if (k * step > 1.0 && std::abs(v) < 1e-18 * std::abs(acc)) break;
+    }
+    return step * acc;
+}
+
+// The ELRA Green's function green_viscous(domain, rho_uppermantle, mean(D))
+// (src/material.jl:370-399, src/tools.jl:53-58): -(L^2 / (2 pi D)) kei(max(R, 1) / L) dx dy,
+// kei(x) = Im K_0(x e^{i pi/4}), L = (D / (rho_m 9.81))^(1/4), on the grid x_i = -W + i dx.
+static std::vector<double> viscous_green(const fi_handle* h) {
+    const size_t n = N2(h);
+    double D = 0.0;
+    for (double d : h->D) D += d;
+    D /= (double)n;
+    const double L = pow(D / (h->cfg.rho_uppermantle * 9.81), 0.25);
+    const std::complex<double> rot = std::polar(1.0, M_PI / 4.0);
+    std::vector<double> G(n);
+    for (int j = 0; j < h->ny; j++)
+        for (int i = 0; i < h->nx; i++) {
+            const double x = -h->cfg.Wx + (i + 1) * h->dx, y = -h->cfg.Wy + (j + 1) * h->dy;
+            const double R = std::max(sqrt(x * x + y * y), 1.0);
+            const double kei = bessel_k0(R / L * rot).imag();
+            G[i + (size_t)j * h->nx] = -(L * L / (2.0 * M_PI * D) * kei) * (h->dx * h->dy);
+        }
+    return G;
+}
+
 static int rhs_fused(fi_handle* h, int stage, const double* uin, float* vout, double* cout);
 static int setup_persist(fi_handle* h, int K);
 static int plan_layouts(fi_handle* h, int K);
@@ -773,6 +840,17 @@ extern "C" int fi_init(fi_handle* h) {
         return set_err(h, FI_ERR_STATE, "ice history not set");
     const bool elastic = c.lithosphere != FI_LITHO_RIGID, geoid = c.sea_surface == FI_SEA_SURFACE_LATERALLY_VARIABLE;
     if (elastic && h->rm.size() < 2) return set_err(h, FI_ERR_STATE, "elastic Green table not set");
+    if (c.mantle < FI_MANTLE_MAXWELL || c.mantle > FI_MANTLE_RIGID || c.alg < FI_ALG_BS3 || c.alg > FI_ALG_EULER ||
+        c.lithosphere < FI_LITHO_LATERALLY_VARIABLE || c.lithosphere > FI_LITHO_LATERALLY_CONSTANT)
+        return set_err(h, FI_ERR_ARG, "unknown mantle, lithosphere or integrator");
+    if (c.mantle == FI_MANTLE_RELAXED && c.lithosphere == FI_LITHO_LATERALLY_VARIABLE)
+        return set_err(h, FI_ERR_UNSUPPORTED, "Relaxed rheology is not implemented for laterally variable lithosphere.");
+    if ((c.alg == FI_ALG_EULER) != (c.dt_min > 0))
+        return set_err(h, FI_ERR_ARG, "The `dt_min` option is only compatible with the Euler algorithm.");
+    if (c.form == FI_FORM_FP32 &&
+        (c.mantle != FI_MANTLE_MAXWELL || c.lithosphere == FI_LITHO_LATERALLY_CONSTANT || c.alg != FI_ALG_BS3))
+        return set_err(h, FI_ERR_UNSUPPORTED, "the FP32 form runs the LV-ELVA path (MaxwellMantle, laterally variable "
+                                              "or rigid lithosphere, BS3); other rheologies run in the plain form");
     if (c.sealevel_load != FI_SEALEVEL_LOAD_NONE && c.sealevel_load != FI_SEALEVEL_LOAD_INTERACTIVE)
         return set_err(h, FI_ERR_ARG, "unknown sea-level load %d", c.sealevel_load);
     if (c.bsl_mode < FI_BSL_CONSTANT || c.bsl_mode > FI_BSL_IMPOSED)
@@ -977,6 +1055,14 @@ extern "C" int fi_init(fi_handle* h) {
         RET(upload(h, p.mgr, mgr0));
         RET(upload(h, p.moc, moc0));
         RET(upload(h, p.hwater, hw0));
+        RET(upload(h, p.tau, h->tau));
+        if (c.mantle == FI_MANTLE_RELAXED) {
+            double* d_Gv = nullptr;
+            RET(dalloc(h, &d_Gv, n));
+            RET(dalloc(h, &p.Gv_hat, (size_t)h->Mx * h->My));
+            RET(upload(h, d_Gv, viscous_green(h)));
+            RET(build_kernel_spectrum(h, d_Gv, nullptr, p.Gv_hat));
+        }
         if (elastic) RET(build_kernel_spectrum(h, h->d_Ge, nullptr, p.Ge_hat));
         if (geoid) RET(build_kernel_spectrum(h, h->d_Gg, nullptr, p.Gg_hat));
         RET(rhs_plain(h, c.t0, p.u[0], p.fscratch));
@@ -1109,7 +1195,8 @@ static int corner_bc_plain(fi_handle* h, double* X, int nx, int ny, double borde
     return FI_OK;
 }
 
-static int conv_plain(fi_handle* h, const double* input, const double2* Ghat, double border, double* output) {
+static int conv_plain(fi_handle* h, const double* input, const double2* Ghat, double border, double* output,
+                      bool regular = false) {
     const size_t M = (size_t)h->Mx * h->My;
     const int cx = 2 * h->nx - 1, cy = 2 * h->ny - 1;
     PlainBufs& p = h->p;
@@ -1121,9 +1208,12 @@ static int conv_plain(fi_handle* h, const double* input, const double2* Ghat, do
     RET(fft2_64(h, p.P, h->Mx, h->My, 1));
     kp_crop<<<gs((size_t)cx * cy), NT, 0, h->stream>>>(p.P, h->Mx, cx, cy, p.cropped);
     CKL();
-    RET(corner_bc_plain(h, p.cropped, cx, cy, border));
+    // samesize_conv! (src/convolutions.jl:134-154): the extended BC space corrects the
+    // (2nx-1) x (2ny-1) result before the crop, the regular one the cropped field
+    if (!regular) RET(corner_bc_plain(h, p.cropped, cx, cy, border));
     kp_window<<<gs(N2(h)), NT, 0, h->stream>>>(p.cropped, cx, h->i1, h->j1, h->nx, h->ny, output);
     CKL();
+    if (regular) RET(corner_bc_plain(h, output, h->nx, h->ny, border));
     return FI_OK;
 }
 
@@ -1215,6 +1305,40 @@ static int rhs_plain(fi_handle* h, double t, double* u, double* dudt) {
     }
     kp_load_full<<<g, NT, 0, h->stream>>>(p.s_i, p.s_sw, p.s_l, p.s_m, p.mask, p.s_load, p.s_full, n);
     CKL();
+    // update_dudt!(dudt, u, sim, t, mantle, lithosphere), src/deformation.jl:21-103
+    if (c.mantle == FI_MANTLE_RIGID) {
+        kp_zero<<<g, NT, 0, h->stream>>>(dudt, n);
+        kp_copy<<<g, NT, 0, h->stream>>>(p.dudt, dudt, n);
+        CKL();
+        return FI_OK;
+    }
+    if (c.mantle == FI_MANTLE_RELAXED) {
+        kp_elra_in<<<g, NT, 0, h->stream>>>(p.s_load, p.s_l, c.g, p.buf, n);
+        CKL();
+        RET(conv_plain(h, p.buf, p.Gv_hat, c.bc_viscous_border, p.u_eq, true));
+        kp_elra_dudt<<<g, NT, 0, h->stream>>>(p.u_eq, p.now_u, p.tau, dudt, n);
+        kp_copy<<<g, NT, 0, h->stream>>>(p.dudt, dudt, n);
+        CKL();
+        return FI_OK;
+    }
+    if (c.lithosphere != FI_LITHO_LATERALLY_VARIABLE) {
+        // one step of dt_min written into u in place; dudt is left as it is
+        kp_lc_in<<<g, NT, 0, h->stream>>>(p.s_load, p.s_l, c.g, u, p.fftrhs, p.fftU, n);
+        CKL();
+        RET(fft2_64(h, p.fftrhs, nx, ny, 0));
+        RET(fft2_64(h, p.fftU, nx, ny, 0));
+        kp_lc_step<<<g, NT, 0, h->stream>>>(p.fftU, p.fftrhs, p.eta, h->d_pd, h->d_R, p.D,
+                                            c.rho_uppermantle * c.g, c.dt_min * c.seconds_per_year, n);
+        CKL();
+        RET(fft2_64(h, p.fftU, nx, ny, 1));
+        kp_real<<<g, NT, 0, h->stream>>>(p.fftU, u, n);
+        CKL();
+        RET(corner_bc_plain(h, u, nx, ny, c.bc_viscous_border));
+        kp_copy<<<g, NT, 0, h->stream>>>(p.now_u, u, n);
+        kp_copy<<<g, NT, 0, h->stream>>>(p.dudt, dudt, n);
+        CKL();
+        return FI_OK;
+    }
     kp_rhs_init<<<g, NT, 0, h->stream>>>(p.s_full, c.g, p.rhs, n);
     CKL();
     kp_dxx<<<g, NT, 0, h->stream>>>(p.bxx, u, nx, ny, h->dx);
@@ -1305,6 +1429,16 @@ static int integ_start(fi_handle* h) {
         }
         RET(read_ctl(h));
         if (h->ctl.status) return set_err(h, h->ctl.status, "%s", fi_status_string(h->ctl.status));
+    } else if (c.alg == FI_ALG_EULER) {
+        // solve(prob, Euler(); dt = dt_min, ...): fsalfirst = f(uprev, t), no initial-dt search
+        RET(rhs_plain(h, ct.t, h->p.u[ct.ibuf], h->p.k14[ct.ik]));
+        h->ctl.dt = c.dt_min;
+        h->ctl.dtpropose = c.dt_min;
+        h->ctl.iter = 0;
+        h->ctl.kout = 0;
+        h->fsal_pending = false;
+        h->integ_started = true;
+        return FI_OK;
     } else {
         PlainBufs& p = h->p;
         RET(rhs_plain(h, ct.t, p.u[ct.ibuf], p.k14[ct.ik]));  // fsalfirst = f(uprev, t)
@@ -1595,6 +1729,15 @@ static int attempt_plain(fi_handle* h) {
     double* un = p.u[ct.ibuf ^ 1];
     double* k1 = p.k14[ct.ik];
     double* k4 = p.k14[ct.ik ^ 1];
+    if (c.alg == FI_ALG_EULER) {
+        // perform_step!(integrator, ::EulerCache): u = uprev + dt k1, k4 = f(u, t + dt)
+        kp_stage<<<gs(n), NT, 0, h->stream>>>(un, up, dt, k1, n);
+        CKL();
+        RET(rhs_plain(h, t + dt, un, k4));
+        euler_accept(&ct, c.dt_min, h->tout.data());
+        ct.nsteps_seg += 1;
+        return FI_OK;
+    }
     kp_stage<<<gs(n), NT, 0, h->stream>>>(p.tmp, up, dt * A21, k1, n);
     CKL();
     RET(rhs_plain(h, t + C2 * dt, p.tmp, p.k2));
@@ -1648,41 +1791,79 @@ struct OutBufs {
     double *t, *u, *ue, *dudt, *dz;
 };
 
+// nout_affect! / write_out! (src/simulation.jl:214-225, src/io.jl:349-353) as an
+// asynchronous pipeline: the output fields are copied on the device into a staging slot
+// (FP32 form: with the corner offsets applied, in FP64) behind the segment that reached
+// the output time; a copy stream reads the slot back into pinned host memory while the
+// next segment runs; the host moves it into the caller's arrays when the slot is reused
+// or when the call ends.  Two slots: at most one output waits while the next is staged.
+static int out_finish(fi_handle* h, int slot) {
+    fi_handle::PendingOut& pd = h->pend[slot];
+    if (!pd.busy) return FI_OK;
+    CK(cudaEventSynchronize(h->ev_copied[slot]));
+    const size_t n = N2(h);
+    for (int f = 0; f < 4; f++)
+        if (pd.dst[f]) memcpy(pd.dst[f] + (size_t)pd.k * n, h->h_out_slot[slot] + (size_t)f * n, n * sizeof(double));
+    pd.busy = false;
+    return FI_OK;
+}
+
+static int out_finish_all(fi_handle* h) {
+    // oldest first: slot of the lower output index
+    int a = 0, b = 1;
+    if (h->pend[1].busy && (!h->pend[0].busy || h->pend[1].k < h->pend[0].k)) { a = 1; b = 0; }
+    RET(out_finish(h, a));
+    RET(out_finish(h, b));
+    return FI_OK;
+}
+
+static int out_setup(fi_handle* h) {
+    if (h->cstream) return FI_OK;
+    const size_t bytes = 4 * N2(h) * sizeof(double);
+    CK(cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking));
+    for (int q = 0; q < 2; q++) {
+        CK(cudaEventCreateWithFlags(&h->ev_staged[q], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->ev_copied[q], cudaEventDisableTiming));
+        CK(cudaMalloc(&h->d_out_slot[q], bytes));
+        CK(cudaMallocHost(&h->h_out_slot[q], bytes));
+    }
+    return FI_OK;
+}
+
 static int record_output(fi_handle* h, int k, const OutBufs& o) {
     const size_t n = N2(h);
     const fi_config& c = h->cfg;
     if (o.t) o.t[k] = h->ctl.t;
+    if (!o.u && !o.ue && !o.dudt && !o.dz) return FI_OK;
+    RET(out_setup(h));
+    const int slot = k & 1;
+    RET(out_finish(h, slot));
+    double* d = h->d_out_slot[slot];
     if (c.form == FI_FORM_FP32) {
         Member& m = h->mem;
         const Ctl& ct = h->ctl;
-        if (o.u) CK(cudaMemcpyAsync(o.u + k * n, m.u[ct.ibuf], n * 8, cudaMemcpyDeviceToHost, h->stream));
-        std::vector<float> v(n);
-        if (o.ue) {
-            CK(cudaMemcpyAsync(v.data(), m.ue[ct.iue], n * 4, cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            const double off = corner_mean(ct.ue_corner[ct.iue]) - c.bc_elastic_border;
-            for (size_t i = 0; i < n; i++) o.ue[k * n + i] = (double)v[i] - off;
-        }
-        if (o.dudt) {
-            CK(cudaMemcpyAsync(v.data(), m.k14[ct.ik], n * 4, cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            const double off = corner_mean(ct.kcorner[ct.ik]) - c.bc_viscous_border;
-            for (size_t i = 0; i < n; i++) o.dudt[k * n + i] = (double)v[i] - off;
-        }
-        if (o.dz) {
-            CK(cudaMemcpyAsync(v.data(), m.dz, n * 4, cudaMemcpyDeviceToHost, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            const double off = corner_mean(ct.dz_corner) - c.bc_sea_surface_border;
-            for (size_t i = 0; i < n; i++) o.dz[k * n + i] = (double)v[i] - off;
-        }
+        const double cue = corner_mean(ct.ue_corner[ct.iue]) - c.bc_elastic_border;
+        const double cdu = corner_mean(ct.kcorner[ct.ik]) - c.bc_viscous_border;
+        const double cdz = corner_mean(ct.dz_corner) - c.bc_sea_surface_border;
+        k_out_stage<<<gs(n), NT, 0, h->stream>>>(o.u ? m.u[ct.ibuf] : nullptr, o.ue ? m.ue[ct.iue] : nullptr, cue,
+                                                 o.dudt ? m.k14[ct.ik] : nullptr, cdu, o.dz ? m.dz : nullptr, cdz,
+                                                 d, n);
+        CKL();
     } else {
         PlainBufs& p = h->p;
-        if (o.u) CK(cudaMemcpyAsync(o.u + k * n, p.now_u, n * 8, cudaMemcpyDeviceToHost, h->stream));
-        if (o.ue) CK(cudaMemcpyAsync(o.ue + k * n, p.ue, n * 8, cudaMemcpyDeviceToHost, h->stream));
-        if (o.dudt) CK(cudaMemcpyAsync(o.dudt + k * n, p.dudt, n * 8, cudaMemcpyDeviceToHost, h->stream));
-        if (o.dz) CK(cudaMemcpyAsync(o.dz + k * n, p.dz, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        const double* src[4] = {p.now_u, p.ue, p.dudt, p.dz};
+        const bool want[4] = {o.u != nullptr, o.ue != nullptr, o.dudt != nullptr, o.dz != nullptr};
+        for (int f = 0; f < 4; f++)
+            if (want[f]) CK(cudaMemcpyAsync(d + (size_t)f * n, src[f], n * 8, cudaMemcpyDeviceToDevice, h->stream));
     }
-    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaEventRecord(h->ev_staged[slot], h->stream));
+    CK(cudaStreamWaitEvent(h->cstream, h->ev_staged[slot], 0));
+    CK(cudaMemcpyAsync(h->h_out_slot[slot], d, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, h->cstream));
+    CK(cudaEventRecord(h->ev_copied[slot], h->cstream));
+    fi_handle::PendingOut& pd = h->pend[slot];
+    pd.busy = true;
+    pd.k = k;
+    pd.dst[0] = o.u; pd.dst[1] = o.ue; pd.dst[2] = o.dudt; pd.dst[3] = o.dz;
     return FI_OK;
 }
 
@@ -1763,9 +1944,10 @@ extern "C" int fi_run(fi_handle* h, int32_t n_out, const double* t_out, double* 
     RET(set_tstops(h, n_out, t_out, true));
     if (h->cfg.form == FI_FORM_FP32) RET(write_ctl(h));
     OutBufs o{out_t, out_u, out_ue, out_dudt, out_dz_ss};
-    RET(solve_until(h, &o));
+    const int rc = solve_until(h, &o);
+    const int rc2 = out_finish_all(h);  // the caller's arrays are complete when fi_run returns
     h->last_call = 0;
-    return FI_OK;
+    return rc ? rc : rc2;
 }
 
 extern "C" int fi_init_integrator(fi_handle* h, int32_t n_tstops, const double* tstops) {
@@ -2349,6 +2531,7 @@ extern "C" int fi_get_field(fi_handle* h, int32_t field, double* host, size_t n)
         case FI_FIELD_UE_REF: v = h->ue_ref; break;
         case FI_FIELD_DZ_SS_REF: v = h->dz_ss_ref; break;
         case FI_FIELD_Z_B_REF: v = h->z_b_ref; break;
+        case FI_FIELD_TAU: v = h->tau; break;
         case FI_FIELD_PSEUDODIFF_SCALING: RET(download(h, v, h->d_R, n)); break;
         case FI_FIELD_PSEUDODIFF: RET(download(h, v, h->d_pd, n)); break;
         case FI_FIELD_SCALED_PSEUDODIFF_INV: RET(download(h, v, h->d_spinv, n)); break;
@@ -2376,6 +2559,7 @@ extern "C" int fi_get_field(fi_handle* h, int32_t field, double* host, size_t n)
                     case FI_FIELD_MASKOCEAN: src = p.moc; break;
                     case FI_FIELD_H_WATER: src = p.hwater; break;
                     case FI_FIELD_COLUMNANOM_SEAWATER: src = p.s_sw; break;
+                    case FI_FIELD_U_EQ: src = p.u_eq; break;
                     default: return set_err(h, FI_ERR_ARG, "unknown field %d", field);
                 }
                 RET(download(h, v, src, n));

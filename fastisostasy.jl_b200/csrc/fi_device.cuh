@@ -157,6 +157,26 @@ __host__ __device__ inline int controller_update_pw(Ctl* c, double EEst, double 
     return c->accept_step;
 }
 
+// Loop footer of a fixed-step Euler step (no error control): always accepted, t
+// snapped to the tstop, the next step back to the fixed dt (clipped again at tstops by
+// loopheader_prep).
+__host__ __device__ inline void euler_accept(Ctl* c, double dt_fixed, const double* tout) {
+    c->EEst = 0.0;
+    c->accept_step = 1;
+    if (c->rec_dt && c->rec_n < c->rec_cap) c->rec_dt[c->rec_n] = c->dt;
+    c->rec_n += 1;
+    c->naccept += 1;
+    const double ttmp = c->t + c->dt;
+    const double ts = c->t_stop;
+    const double big = c->t > ts ? c->t : ts;
+    c->t = (fabs(ttmp - ts) < 100.0 * ulp_above(big)) ? ts : ttmp;
+    c->dtpropose = dt_fixed;
+    c->dt = dt_fixed;
+    c->ibuf ^= 1;
+    c->ik ^= 1;
+    if (c->kout < c->nout && c->t >= tout[c->kout]) c->pending_output = 1;
+}
+
 __host__ __device__ inline int controller_update(Ctl* c, double EEst, const double* tout) {
     const bool pw = (EEst == EEst) && EEst != 0.0;
     return controller_update_pw(c, EEst, pw ? pow(EEst, PI_BETA1) : 0.0, pw ? pow(c->qold, PI_BETA2) : 1.0, tout);

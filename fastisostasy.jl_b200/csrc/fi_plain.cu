@@ -262,4 +262,48 @@ __global__ void kp_initdt_terms(const double* f0, const double* f1, const double
     if (threadIdx.x == 0) { partial[2 * blockIdx.x] = v[0]; partial[2 * blockIdx.x + 1] = v[1]; }
 }
 
+// ELRA (src/deformation.jl:29-45): the convolution input -(load + litho) g K^2 and
+// dudt = (u_eq - u) / tau
+__global__ void kp_elra_in(const double* s_load, const double* s_l, double g, double* out, size_t n) {
+    GRID_STRIDE(i, n) out[i] = -(s_load[i] + s_l[i]) * g;
+}
+__global__ void kp_elra_dudt(const double* u_eq, const double* u, const double* tau, double* dudt, size_t n) {
+    GRID_STRIDE(i, n) dudt[i] = 1.0 / tau[i] * (u_eq[i] - u[i]);
+}
+
+// Laterally-constant Maxwell step (src/deformation.jl:52-89): F = -(load + litho) g,
+// U = u as complex inputs; then U <- ((nabla - dt/2 beta) U + dt F) / (nabla + dt/2 beta)
+// with nabla = 2 eta |k| R and beta = rho_m g + D |k|^4, elementwise as the reference
+// broadcasts them; then u = Re(ifft(U)).
+__global__ void kp_lc_in(const double* s_load, const double* s_l, double g, const double* u, double2* F, double2* U,
+                         size_t n) {
+    GRID_STRIDE(i, n) {
+        F[i] = make_double2(-(s_load[i] + s_l[i]) * g, 0.0);
+        U[i] = make_double2(u[i], 0.0);
+    }
+}
+__global__ void kp_lc_step(double2* U, const double2* F, const double* eta, const double* pd, const double* R,
+                           const double* D, double rho_m_g, double dt, size_t n) {
+    GRID_STRIDE(i, n) {
+        const double k = pd[i];
+        const double nab = 2.0 * eta[i] * k * R[i];
+        const double beta = rho_m_g + D[i] * k * k * k * k;
+        const double a = nab - dt / 2 * beta, b = nab + dt / 2 * beta;
+        U[i] = make_double2((a * U[i].x + dt * F[i].x) / b, (a * U[i].y + dt * F[i].y) / b);
+    }
+}
+__global__ void kp_real(const double2* U, double* u, size_t n) { GRID_STRIDE(i, n) u[i] = U[i].x; }
+
+// Output staging of the FP32 form: out = [u | ue - cue | dudt - cdu | dz - cdz] in FP64
+// (fields whose source is null are skipped).
+__global__ void k_out_stage(const double* u, const float* ue, double cue, const float* dudt, double cdu,
+                            const float* dz, double cdz, double* out, size_t n) {
+    GRID_STRIDE(i, n) {
+        if (u) out[i] = u[i];
+        if (ue) out[n + i] = (double)ue[i] - cue;
+        if (dudt) out[2 * n + i] = (double)dudt[i] - cdu;
+        if (dz) out[3 * n + i] = (double)dz[i] - cdz;
+    }
+}
+
 }  // namespace fi

@@ -46,4 +46,13 @@ __global__ void kp_norms2(const double* a, const double* b, const double* sk_bas
                           double* partial, size_t n);
 __global__ void kp_initdt_terms(const double* f0, const double* f1, const double* sk_base, double abstol,
                                 double reltol, double* partial, size_t n);
+__global__ void kp_elra_in(const double* s_load, const double* s_l, double g, double* out, size_t n);
+__global__ void kp_elra_dudt(const double* u_eq, const double* u, const double* tau, double* dudt, size_t n);
+__global__ void kp_lc_in(const double* s_load, const double* s_l, double g, const double* u, double2* F, double2* U,
+                         size_t n);
+__global__ void kp_lc_step(double2* U, const double2* F, const double* eta, const double* pd, const double* R,
+                           const double* D, double rho_m_g, double dt, size_t n);
+__global__ void kp_real(const double2* U, double* u, size_t n);
+__global__ void k_out_stage(const double* u, const float* ue, double cue, const float* dudt, double cdu,
+                            const float* dz, double cdz, double* out, size_t n);
 }  // namespace fi

@@ -267,10 +267,14 @@ class SolidEarth:
         self.compressibility = compressibility or CompressibleMantle()
         self.lumping = lumping or FreqDomainViscosityLumping()
         self.lithosphere_column = lithosphere_column or IncompressibleLithosphereColumn()
-        if self.mantle != MaxwellMantle():
-            raise UnsupportedError(f"{self.mantle!r}: only MaxwellMantle is on the LV-ELVA path")
-        if self.lithosphere not in (LaterallyVariableLithosphere(), RigidLithosphere()):
-            raise UnsupportedError(f"{self.lithosphere!r} selects the implicit laterally-constant solver")
+        if self.mantle not in (MaxwellMantle(), RelaxedMantle(), RigidMantle()):
+            raise UnsupportedError(f"mantle {self.mantle!r}")
+        if self.lithosphere not in (LaterallyVariableLithosphere(), LaterallyConstantLithosphere(),
+                                    RigidLithosphere()):
+            raise UnsupportedError(f"lithosphere {self.lithosphere!r}")
+        if self.mantle == RelaxedMantle() and self.lithosphere == LaterallyVariableLithosphere():
+            # src/deformation.jl:47-50
+            raise UnsupportedError("Relaxed rheology is not implemented for laterally variable lithosphere.")
         if self.lumping != FreqDomainViscosityLumping():
             raise UnsupportedError(f"{self.lumping!r}: only FreqDomainViscosityLumping is supported")
         nx, ny = domain.nx, domain.ny
@@ -444,8 +448,16 @@ class Simulation:
         self.c = c or PhysicalConstants()
         self.nout = nout or NativeOutput()
         self.t_span = (float(t_span[0]), float(t_span[1]))
-        if self.opts.diffeq.alg != "BS3" or self.opts.diffeq.dt_min is not None:
-            raise UnsupportedError("only the adaptive BS3 default of run! is on the hot path")
+        dq = self.opts.diffeq
+        if dq.alg not in ("BS3", "Euler"):
+            raise UnsupportedError(f"integrator {dq.alg!r}: BS3 (adaptive) or Euler (fixed dt_min)")
+        if (dq.dt_min is not None) != (dq.alg == "Euler"):
+            # src/simulation.jl:244-256
+            raise UnsupportedError("The `dt_min` option is only compatible with the Euler algorithm.")
+        if form == "fp32" and (dq.alg != "BS3" or solidearth.mantle != MaxwellMantle()
+                               or solidearth.lithosphere == LaterallyConstantLithosphere()):
+            raise UnsupportedError("the FP32 form runs the LV-ELVA path (MaxwellMantle, laterally variable or rigid "
+                                   "lithosphere, BS3); other rheologies run in the plain FP64 form (form='fp64')")
         nx, ny = domain.nx, domain.ny
         z = domain.zeros
         self.u_ref = z() if u_ref is None else np.asarray(u_ref, float)
@@ -460,8 +472,13 @@ class Simulation:
         cfg.rho_ice, cfg.rho_water, cfg.rho_seawater = c_.rho_ice, c_.rho_water, c_.rho_seawater
         cfg.rho_litho, cfg.rho_uppermantle = solidearth.rho_litho, solidearth.rho_uppermantle
         cfg.litho_poissonratio = solidearth.litho_poissonratio
-        cfg.lithosphere = (abi.FI_LITHO_RIGID if solidearth.lithosphere == RigidLithosphere()
-                           else abi.FI_LITHO_LATERALLY_VARIABLE)
+        cfg.lithosphere = {RigidLithosphere(): abi.FI_LITHO_RIGID,
+                           LaterallyConstantLithosphere(): abi.FI_LITHO_LATERALLY_CONSTANT}.get(
+            solidearth.lithosphere, abi.FI_LITHO_LATERALLY_VARIABLE)
+        cfg.mantle = {RelaxedMantle(): abi.FI_MANTLE_RELAXED, RigidMantle(): abi.FI_MANTLE_RIGID}.get(
+            solidearth.mantle, abi.FI_MANTLE_MAXWELL)
+        cfg.alg = abi.FI_ALG_EULER if dq.alg == "Euler" else abi.FI_ALG_BS3
+        cfg.dt_min = float(dq.dt_min) if dq.dt_min is not None else 0.0
         cfg.lithosphere_column = (abi.FI_COLUMN_COMPRESSIBLE
                                   if solidearth.lithosphere_column == CompressibleLithosphereColumn()
                                   else abi.FI_COLUMN_INCOMPRESSIBLE)
@@ -520,6 +537,7 @@ class Simulation:
             "litho_rigidity": se.litho_rigidity,
             "effective_viscosity": se.effective_viscosity,
             "maskactive": se.maskactive.astype(np.float64),
+            "tau": se.tau,
             "u_ref": self.u_ref,
             "ue_ref": self.ue_ref,
             "dz_ss_ref": self.dz_ss_ref,

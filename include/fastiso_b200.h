@@ -57,7 +57,14 @@ enum {
 };
 
 /* ---- tags of the reference (src/solidearth.jl:13-109, src/sealevel.jl:114-130) ---- */
-enum { FI_LITHO_LATERALLY_VARIABLE = 0, FI_LITHO_RIGID = 1 };
+enum { FI_LITHO_LATERALLY_VARIABLE = 0, FI_LITHO_RIGID = 1, FI_LITHO_LATERALLY_CONSTANT = 2 };
+/* solidearth.mantle (src/solidearth.jl:40-75): MaxwellMantle (the LV-ELVA default),
+ * RelaxedMantle (ELRA: dudt = (u_eq - u) / tau with u_eq the Kelvin-function
+ * convolution of the load, src/deformation.jl:29-45), RigidMantle (dudt = 0). */
+enum { FI_MANTLE_MAXWELL = 0, FI_MANTLE_RELAXED = 1, FI_MANTLE_RIGID = 2 };
+/* opts.diffeq.alg: BS3 (adaptive) or Euler with the fixed step dt_min, which the
+ * laterally-constant Maxwell form needs (src/simulation.jl:236-262). */
+enum { FI_ALG_BS3 = 0, FI_ALG_EULER = 1 };
 enum { FI_SEA_SURFACE_LATERALLY_CONSTANT = 0, FI_SEA_SURFACE_LATERALLY_VARIABLE = 1 };
 enum { FI_COLUMN_INCOMPRESSIBLE = 0, FI_COLUMN_COMPRESSIBLE = 1 };
 enum { FI_ICE_TIME_INTERPOLATED = 0, FI_ICE_EXTERNAL = 1 };
@@ -102,6 +109,10 @@ typedef struct fi_config {
     int32_t density_contribution;   /* FI_CONTRIB_NONE or FI_CONTRIB_GOELZER */
     int32_t adjustment_contribution;/* FI_CONTRIB_NONE or FI_CONTRIB_GOELZER */
     double bsl_ref_A;               /* ReferenceBSL ocean area ref.A (m^2), A_OCEAN_PD = 3.625e14 */
+    /* rheology and integrator beyond the LV-ELVA path (the plain FP64 form runs them) */
+    int32_t mantle;                 /* FI_MANTLE_* */
+    int32_t alg;                    /* FI_ALG_* */
+    double dt_min;                  /* DiffEqOptions dt_min (yr) of FI_ALG_EULER */
 } fi_config;
 
 /* sealevel.load (src/loads.jl:1-27) */
@@ -144,7 +155,9 @@ enum {
     FI_FIELD_MASKOCEAN = 23,          /* sim.now.maskocean as 0/1 (get) */
     FI_FIELD_H_WATER = 24,            /* sim.now.H_water (get) */
     FI_FIELD_COLUMNANOM_SEAWATER = 25,/* sim.now.columnanoms.seawater (get) */
-    FI_NUM_FIELDS = 26
+    FI_FIELD_TAU = 26,                /* SolidEarth.tau, ELRA relaxation time in yr (set; default 855) */
+    FI_FIELD_U_EQ = 27,               /* sim.now.u_eq, ELRA equilibrium displacement (get) */
+    FI_NUM_FIELDS = 28
 };
 
 /* Barystatic sea level and the volume terms of the last sparse update (sim.now.z_bsl,

@@ -19,6 +19,8 @@
  */
 #include "fi_oracle.h"
 
+#include <complex.h>
+#undef I /* the integrator variables are named I; the imaginary unit is _Complex_I */
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -196,6 +198,8 @@ typedef struct {
     int status;
     /* step-sequence replay / record (same semantics as the library's
        fi_set_step_replay / fi_record_steps) */
+    int euler;          /* Euler with the fixed step dt_fixed (dt_min), no error control */
+    double dt_fixed;
     double* replay;
     int64_t replay_n, replay_i;
     double* rec;
@@ -231,6 +235,10 @@ struct or_sim {
     /* sea level beyond the surface (src/sealevel.jl:242-332, src/barystatic_sealevel.jl) */
     double z_bsl, A_bsl, V_af, V_den, V_pov, delta_V;
     double *H_water, *mask_gr, *mask_oc;
+    /* other rheologies (src/deformation.jl:29-89): ELRA relaxation time, equilibrium
+       displacement and the viscous (Kelvin-function) Green's function */
+    double *tau, *u_eq, *Gv;
+    cpx *Gv_hat, *fftU;
     int n_osurf, n_bslh;
     double *osurf_z, *osurf_A, *bslh_t, *bslh_z;
     /* work buffers */
@@ -361,6 +369,42 @@ static void pad_to(cpx* P, const double* in, int nx, int ny, int Mx, int My) {
 }
 
 /* kernel_fft = p_rfft * pad(kernel) (full complex spectrum here) */
+/* K_0(z) for complex z with Re z > 0 (SpecialFunctions besselk(0, z) as the reference
+ * calls it) from the integral K_0(z) = int_0^inf exp(-z cosh t) dt (Abramowitz &
+ * Stegun 9.6.24) by the trapezoidal rule with step 1/20: the integrand is analytic and
+ * decays doubly exponentially, so the rule converges geometrically (about 1e-15 relative
+ * for |z| in [1e-5, 60] on the ray arg z = pi/4, checked against scipy). */
+static double complex besselk0_(double complex z) {
+    const double h = 0.05;
+    double complex sum = 0.5 * cexp(-z);
+    for (int k = 1; k < 4000; k++) {
+        const double complex v = cexp(-z * cosh(k * h));
+        sum += v;
+        if (k * h > 1.0 && cabs(v) < 1e-18 * cabs(sum)) break;
+    }
+    return h * sum;
+}
+
+/* besselkei(x) = imag(besselk(0, x e^{i pi/4})), src/material.jl:370-373 */
+double or_kei(double x) { return cimag(besselk0_(x * cexp(_Complex_I * M_PI / 4.0))); }
+
+/* green_viscous(domain, rho_uppermantle, mean(litho_rigidity)) (src/material.jl:375-380,
+ * src/tools.jl:53-58): -(L^2 / (2 pi D)) kei(max(R, 1) / L) dx dy with the flexural
+ * length L = (D / (rho g))^(1/4), g = 9.81 (src/material.jl:396-399). */
+static void build_viscous_green_(or_sim* s) {
+    const size_t n = (size_t)s->nx * s->ny;
+    double D = 0.0;
+    for (size_t k = 0; k < n; k++) D += s->D[k];
+    D /= (double)n;
+    const double L = pow(D / (s->cfg.rho_uppermantle * 9.81), 0.25);
+    for (int j = 0; j < s->ny; j++)
+        for (int i = 0; i < s->nx; i++) {
+            double R = sqrt(s->x[i] * s->x[i] + s->y[j] * s->y[j]);
+            if (R < 1.0) R = 1.0;
+            s->Gv[i + (size_t)j * s->nx] = -(L * L / (2.0 * M_PI * D) * or_kei(R / L)) * (s->dx * s->dy);
+        }
+}
+
 static void conv_plan(or_sim* s, const double* kernel, cpx* khat) {
     pad_to(khat, kernel, s->nx, s->ny, s->Mx, s->My);
     fft2(&s->fMx, &s->fMy, khat, s->Mx, s->My, 0);
@@ -527,9 +571,11 @@ int or_create(const fi_config* cfg, or_sim** out) {
                          &s->z_ss_ref, &s->u, &s->ue, &s->dudt, &s->H_ice, &s->H_af, &s->z_b, &s->dz_ss,
                          &s->z_ss, &s->c_ice, &s->c_sw, &s->c_sed, &s->c_litho, &s->c_mantle, &s->c_load,
                          &s->c_full, &s->rhs, &s->bxx, &s->byy, &s->bx, &s->bxy, &s->Mxx, &s->Myy, &s->Mxy,
-                         &s->buf, &s->H_water, &s->mask_gr, &s->mask_oc};
+                         &s->buf, &s->H_water, &s->mask_gr, &s->mask_oc, &s->tau, &s->u_eq, &s->Gv};
     for (size_t k = 0; k < sizeof(fields) / sizeof(fields[0]); k++) *fields[k] = dalloc(n);
-    for (size_t k = 0; k < n; k++) { s->R[k] = 1.0; s->mask[k] = 1.0; s->z_b_ref[k] = 1e6; }
+    for (size_t k = 0; k < n; k++) { s->R[k] = 1.0; s->mask[k] = 1.0; s->z_b_ref[k] = 1e6; s->tau[k] = 855.0; }
+    s->Gv_hat = (cpx*)calloc(M, sizeof(cpx));
+    s->fftU = (cpx*)calloc(n, sizeof(cpx));
     s->fftrhs = (cpx*)calloc(n, sizeof(cpx));
     s->convbuf = (cpx*)calloc(M, sizeof(cpx));
     s->Ge_hat = (cpx*)calloc(M, sizeof(cpx));
@@ -547,9 +593,9 @@ void or_destroy(or_sim* s) {
                       s->c_sed, s->c_litho, s->c_mantle, s->c_load, s->c_full, s->rhs, s->bxx, s->byy, s->bx,
                       s->bxy, s->Mxx, s->Myy, s->Mxy, s->buf, s->cropped, s->rm, s->GE, s->t_ice, s->H_tab,
                       s->ch_ratio, s->ch_thick, s->tout_copy, s->H_water, s->mask_gr, s->mask_oc,
-                      s->osurf_z, s->osurf_A, s->bslh_t, s->bslh_z};
+                      s->osurf_z, s->osurf_A, s->bslh_t, s->bslh_z, s->tau, s->u_eq, s->Gv};
     for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); k++) free(ptrs[k]);
-    free(s->fftrhs); free(s->convbuf); free(s->Ge_hat); free(s->Gg_hat);
+    free(s->fftrhs); free(s->convbuf); free(s->Ge_hat); free(s->Gg_hat); free(s->Gv_hat); free(s->fftU);
     fft_plan_free(&s->fx); fft_plan_free(&s->fy); fft_plan_free(&s->fMx); fft_plan_free(&s->fMy);
     or_integ* I = &s->I;
     free(I->u); free(I->uprev); free(I->k1); free(I->k2); free(I->k3); free(I->k4); free(I->tmp);
@@ -587,6 +633,8 @@ static double* field_ptr(or_sim* s, int32_t f, int for_set) {
         case FI_FIELD_MASKOCEAN: return for_set ? NULL : s->mask_oc;
         case FI_FIELD_H_WATER: return for_set ? NULL : s->H_water;
         case FI_FIELD_COLUMNANOM_SEAWATER: return for_set ? NULL : s->c_sw;
+        case FI_FIELD_TAU: return s->tau;
+        case FI_FIELD_U_EQ: return for_set ? NULL : s->u_eq;
         default: return NULL;
     }
 }
@@ -860,6 +908,60 @@ static int rhs_impl(or_sim* s, double t, double* u, double* dudt) {
         s->c_load[k] = s->mask[k] * (s->c_ice[k] + s->c_sw[k] + s->c_sed[k]);
         s->c_full[k] = s->c_load[k] + s->mask[k] * (s->c_litho[k] + s->c_mantle[k]);
     }
+    /* update_dudt!(dudt, u, sim, t, mantle, lithosphere), src/deformation.jl:21-103 */
+    if (c->mantle == FI_MANTLE_RIGID) {
+        memset(dudt, 0, n * sizeof(double)); /* RigidMantle: dudt .= 0 */
+        memcpy(s->dudt, dudt, n * sizeof(double));
+        return FI_OK;
+    }
+    if (c->mantle == FI_MANTLE_RELAXED) {
+        if (c->lithosphere == FI_LITHO_LATERALLY_VARIABLE)
+            return set_err(s, FI_ERR_UNSUPPORTED,
+                           "Relaxed rheology is not implemented for laterally variable lithosphere.");
+        /* ELRA (src/deformation.jl:29-45): u_eq = samesize_conv(-(load + litho) g K^2,
+         * viscous Green) in the regular BC space, dudt = (u_eq - u) / tau */
+        const int cx = 2 * nx - 1;
+        for (size_t k = 0; k < n; k++) s->buf[k] = -(s->c_load[k] + s->c_litho[k]) * c->g;
+        conv_full_(s, s->buf, s->Gv_hat, s->cropped);
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++)
+                s->u_eq[i + (size_t)j * nx] = s->cropped[(s->i1 - 1 + i) + (size_t)(s->j1 - 1 + j) * cx];
+        corner_bc(s->u_eq, nx, ny, c->bc_viscous_border);
+        for (size_t k = 0; k < n; k++) dudt[k] = 1.0 / s->tau[k] * (s->u_eq[k] - s->u[k]);
+        memcpy(s->dudt, dudt, n * sizeof(double));
+        for (size_t k = 0; k < n; k++)
+            if (!isfinite(dudt[k])) return set_err(s, FI_ERR_NONFINITE, "non-finite dudt");
+        return FI_OK;
+    }
+    if (c->lithosphere != FI_LITHO_LATERALLY_VARIABLE) {
+        /* MaxwellMantle with a laterally constant or rigid lithosphere (Bueler et al. 2007,
+         * src/deformation.jl:52-89): one step of dt_min of the spectral scheme
+         * U+ = ((nabla - dt/2 beta) U + dt F) / (nabla + dt/2 beta), nabla = 2 eta |k| R,
+         * beta = rho_m g + D |k|^4, written into u in place; dudt is left as it is */
+        const double dt = c->dt_min * c->seconds_per_year;
+        for (size_t k = 0; k < n; k++) {
+            s->fftrhs[k].re = -(s->c_load[k] + s->c_litho[k]) * c->g; /* K == 1 */
+            s->fftrhs[k].im = 0.0;
+            s->fftU[k].re = u[k];
+            s->fftU[k].im = 0.0;
+        }
+        fft2(&s->fx, &s->fy, s->fftrhs, nx, ny, 0);
+        fft2(&s->fx, &s->fy, s->fftU, nx, ny, 0);
+        for (size_t k = 0; k < n; k++) {
+            const double pd = s->pseudodiff[k];
+            const double nab = 2.0 * s->eta[k] * pd * s->R[k];
+            const double beta = c->rho_uppermantle * c->g + s->D[k] * pd * pd * pd * pd;
+            const double a = nab - dt / 2 * beta, b = nab + dt / 2 * beta;
+            s->fftU[k].re = (a * s->fftU[k].re + dt * s->fftrhs[k].re) / b;
+            s->fftU[k].im = (a * s->fftU[k].im + dt * s->fftrhs[k].im) / b;
+        }
+        fft2(&s->fx, &s->fy, s->fftU, nx, ny, 1);
+        for (size_t k = 0; k < n; k++) u[k] = s->fftU[k].re;
+        corner_bc(u, nx, ny, c->bc_viscous_border);
+        memcpy(s->u, u, n * sizeof(double));
+        memcpy(s->dudt, dudt, n * sizeof(double));
+        return FI_OK;
+    }
     /* update_dudt!(.., MaxwellMantle, LaterallyVariableLithosphere), deformation.jl:91-103 */
     /* update_deformation_rhs!(sim, u), deformation.jl:110-131 */
     const double nu = c->litho_poissonratio;
@@ -926,6 +1028,10 @@ static int setup_(or_sim* s) {
     }
     build_geoid_green_(s);
     conv_plan(s, s->Gg, s->Gg_hat);
+    if (c->mantle == FI_MANTLE_RELAXED) {
+        build_viscous_green_(s);
+        conv_plan(s, s->Gv, s->Gv_hat);
+    }
     /* reference state, src/simulation.jl:132-151 */
     memset(s->H_ice_ref, 0, n * sizeof(double));
     if (c->ice_mode == FI_ICE_TIME_INTERPOLATED) {
@@ -1063,6 +1169,13 @@ static int integ_start(or_integ* I, const double* u0, double t0, double t1) {
     /* initialize!(integrator, ::BS3Cache): fsalfirst = f(uprev, t) */
     int rc = I->f(I->ctx, t0, I->uprev, I->k1);
     if (rc) return rc;
+    if (I->euler) {
+        /* solve(prob, Euler(); dt = dt_min, dtmin = dt_min, force_dtmin = true) */
+        I->dt = I->dt_fixed;
+        I->dtpropose = I->dt_fixed;
+        I->initialized = 1;
+        return FI_OK;
+    }
     /* handle_dt! -> auto_dt_reset! -> ode_determine_initdt */
     double* sk = I->tmp;
     for (int k = 0; k < n; k++) sk[k] = I->abstol + fabs(I->u[k]) * I->reltol;
@@ -1157,6 +1270,40 @@ static int integ_attempt(or_integ* I) {
     if (I->max_steps > 0 && I->iter > I->max_steps) return FI_ERR_MAXITERS;
     if (!(I->dt == I->dt)) return FI_ERR_NONFINITE;
     if (I->dt <= I->dtmin) return FI_ERR_DT_UNDERFLOW;
+    if (I->euler) {
+        /* fixed step: the next attempt restarts from dt_min (dtcache), clipped at tstops */
+        if (I->iter > 1 && !(I->replay_n > 0 && I->replay_i <= I->replay_n)) {
+            I->dt = I->dt_fixed;
+            if (I->ntstops > 0 && I->tstops[0] - I->t < I->dt) I->dt = I->tstops[0] - I->t;
+        }
+        /* perform_step!(integrator, ::EulerCache): u = uprev + dt k1; k4 = f(u, t + dt) (FSAL) */
+        const double t = I->t, dt = I->dt;
+        for (int k = 0; k < n; k++) I->u[k] = I->uprev[k] + dt * I->k1[k];
+        if ((rc = I->f(I->ctx, t + dt, I->u, I->k4))) return rc;
+        I->EEst = 0.0;
+        I->reeval_fsal = 0;
+        I->u_modified = 0;
+        const double ttmp = I->t + I->dt;
+        I->accept_step = 1;
+        if (I->rec && I->rec_n < I->rec_cap) I->rec[I->rec_n] = I->dt;
+        I->rec_n++;
+        I->naccept++;
+        if (I->ntstops > 0) {
+            const double ts = I->tstops[0];
+            const double big = I->t > ts ? I->t : ts;
+            I->t = (fabs(ttmp - ts) < 100 * eps_(big)) ? ts : ttmp;
+        } else {
+            I->t = ttmp;
+        }
+        I->dtpropose = I->dt_fixed;
+        if (I->nout > 0 && I->kout < I->nout && I->t >= I->tout[I->kout]) {
+            if (I->record) I->record(I->ctx, I->kout, I->t);
+            I->kout++;
+            I->u_modified = 1;
+            I->reeval_fsal = 1;
+        }
+        return FI_OK;
+    }
     /* perform_step!(integrator, ::BS3Cache) */
     const double t = I->t, dt = I->dt;
     for (int k = 0; k < n; k++) I->tmp[k] = I->uprev[k] + dt * BS3_A21 * I->k1[k];
@@ -1279,6 +1426,10 @@ static int start_integrator_at_(or_sim* s, double t_start, int32_t n_tstops, con
     I->ctx = s;
     I->reltol = s->cfg.reltol;
     I->abstol = s->cfg.abstol;
+    I->euler = s->cfg.alg == FI_ALG_EULER;
+    I->dt_fixed = s->cfg.dt_min;
+    if (I->euler && !(I->dt_fixed > 0))
+        return set_err(s, FI_ERR_ARG, "The `dt_min` option is only compatible with the Euler algorithm.");
     I->max_steps = s->cfg.max_steps;
     I->record = record_;
     I->kout = 0;

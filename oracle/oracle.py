@@ -56,6 +56,7 @@ def lib():
         "or_destroy": (None, [C.c_void_p]),
         "or_set_threads": (None, [C.c_int32]),
         "or_nextfastfft": (C.c_int32, [C.c_int32]),
+        "or_kei": (C.c_double, [C.c_double]),
         "or_second_derivatives": (None, [C.c_int32, C.c_int32, C.c_double, C.c_double, dp, dp, dp, dp, dp]),
         "or_fft2": (C.c_int, [C.c_int32, C.c_int32, dp, dp, dp, dp, C.c_int32]),
         "or_conv_full": (C.c_int, [C.c_int32, C.c_int32, dp, dp, dp]),
@@ -233,6 +234,11 @@ def conv_full(kernel2d, input2d):
     out = np.empty((2 * ny - 1) * (2 * nx - 1))
     lib().or_conv_full(nx, ny, _p(k), _p(x), _p(out))
     return out.reshape(2 * ny - 1, 2 * nx - 1).T
+
+
+def kei(x: float) -> float:
+    """The Kelvin function kei of the oracle's ELRA Green's function."""
+    return float(lib().or_kei(float(x)))
 
 
 def nextfastfft(n: int) -> int:

@@ -185,3 +185,64 @@ def test_oracle_resume_continues_the_run():
     b.step(300.0)
     assert rel_l2(b.get_field(8), a.get_field(8)) < 2e-3
     assert b.stats()["nsparse"] >= st["nsparse"] + 29
+
+
+def test_kei_matches_scipy():
+    """The Kelvin function of the ELRA Green's function, imag(besselk(0, x e^{i pi/4}))
+    as src/material.jl:370-373 defines it, against scipy's complex K_0 (AMOS) to 1e-13
+    of |K_0|, and against scipy.special.kei (a separate algorithm, ~1e-11 here) to 1e-9."""
+    for x in (1e-5, 1e-3, 0.1, 0.5, 1.0, 2.0, 5.0, 7.9, 8.1, 12.0, 20.0, 40.0):
+        k0 = scipy.special.kv(0, x * np.exp(1j * np.pi / 4))
+        assert abs(O.kei(x) - k0.imag) <= 1e-13 * abs(k0), (x, O.kei(x), k0)
+        assert abs(O.kei(x) - scipy.special.kei(x)) <= 1e-9 * abs(k0), x
+
+
+def test_analytic_disc_load_laterally_constant_maxwell():
+    """The laterally-constant Maxwell scheme (src/deformation.jl:52-89, Bueler et al.
+    2007) with Euler steps of dt_min = 10 yr follows the same analytic disc-load
+    solution as the LV-ELVA solve."""
+    domain = F.RegionalDomain(3e6, 7)
+    H1 = 1e3 * (domain.R < 1e6)
+    it = F.TimeInterpolatedIceThickness([0.0, 1.0, 50e3], [domain.zeros(), H1, H1], domain)
+    bcs = F.BoundaryConditions(domain, ice_thickness=it)
+    se = F.SolidEarth(domain, layer_boundaries=[88e3], layer_viscosities=[1e21], rho_litho=0.0,
+                      lithosphere=F.LaterallyConstantLithosphere())
+    t_check = [5e3, 10e3]
+    opts = F.SolverOptions(diffeq=F.DiffEqOptions(alg="Euler", dt_min=10.0))
+    sim = F.Simulation(domain, bcs, F.RegionalSeaLevel(), se, (0.0, 10e3), nout=F.NativeOutput(t=t_check),
+                       form="fp64", opts=opts)
+    ref = oracle_for(sim)
+    ref.init()
+    out = ref.run(np.asarray(t_check), want=("u",))
+    j = domain.my - 1
+    xs = domain.x[domain.mx - 1:]
+    c = F.PhysicalConstants()
+    D = float(np.mean(se.litho_rigidity))
+    eta = float(np.mean(se.effective_viscosity))
+    for k, t in enumerate(t_check):
+        u = out["u"][k].reshape(domain.ny, domain.nx).T
+        num = u[domain.mx - 1:, j]
+        ana = np.array([analytic_solution(abs(x), t * c.seconds_per_year, c.rho_ice, c.g, se.rho_uppermantle, D,
+                                          eta) for x in xs])
+        assert rel_l2(num, ana) < 0.03, (t, rel_l2(num, ana))
+
+
+def test_elra_relaxes_to_equilibrium():
+    """ELRA (src/deformation.jl:29-45): with a constant load the displacement relaxes to
+    the equilibrium u_eq = Kelvin-function convolution of the load, dudt = (u_eq - u)/tau."""
+    domain = F.RegionalDomain(1.5e6, 1.5e6, 48, 48)
+    H1 = 1e3 * (domain.R < 5e5)
+    it = F.TimeInterpolatedIceThickness([0.0, 1.0, 20e3], [domain.zeros(), H1, H1], domain)
+    bcs = F.BoundaryConditions(domain, ice_thickness=it)
+    se = F.SolidEarth(domain, layer_boundaries=[100e3], layer_viscosities=[1e21], mantle=F.RelaxedMantle(),
+                      lithosphere=F.LaterallyConstantLithosphere(), tau=300.0)
+    sim = F.Simulation(domain, bcs, F.RegionalSeaLevel(), se, (0.0, 6e3), nout=F.NativeOutput(t=[6e3]),
+                       form="fp64")
+    ref = oracle_for(sim)
+    ref.init()
+    out = ref.run(np.asarray([6e3]), want=("u", "dudt"))
+    u_eq = ref.get_field(F.abi.FIELDS["u_eq"])
+    assert u_eq.min() < -100.0
+    assert rel_l2(out["u"][0], u_eq) < 1e-4
+    np.testing.assert_allclose(ref.get_field(F.abi.FIELDS["dudt"]), (u_eq - ref.get_field(8)) / 300.0, rtol=1e-10,
+                               atol=1e-12)

@@ -17,7 +17,8 @@ const FI_FORM_FP64 = Int32(1)
 # field ids (fi_set_field / fi_get_field)
 const F = (litho_rigidity = 0, effective_viscosity = 1, pseudodiff_scaling = 2, maskactive = 3,
            u_ref = 4, ue_ref = 5, dz_ss_ref = 6, z_b_ref = 7, u = 8, ue = 9, dudt = 10, dz_ss = 11,
-           H_ice = 12, z_ss = 13, z_b = 14)
+           H_ice = 12, z_ss = 13, z_b = 14, H_af = 21, maskgrounded = 22, maskocean = 23, H_water = 24,
+           columnanom_seawater = 25, tau = 26, u_eq = 27)
 
 # fi_config, field for field (isbits: Julia lays it out as C does)
 mutable struct FiConfig
@@ -33,10 +34,15 @@ mutable struct FiConfig
     t0::Float64; t1::Float64; reltol::Float64; abstol::Float64; dt_sparse_diagnostics::Float64
     max_steps::Int64
     form::Int32; device::Int32
+    sealevel_load::Int32; bsl_mode::Int32; bsl_update::Int32
+    volume_contribution::Int32; density_contribution::Int32; adjustment_contribution::Int32
+    bsl_ref_A::Float64
+    mantle::Int32; alg::Int32
+    dt_min::Float64
 end
 
 FiConfig() = FiConfig(zeros(Int32, 2)..., zeros(12)..., zeros(Int32, 3)..., zeros(4)..., zeros(Int32, 2)...,
-                      zeros(5)..., Int64(0), Int32(0), Int32(0))
+                      zeros(5)..., Int64(0), Int32(0), Int32(0), zeros(Int32, 6)..., 0.0, Int32(0), Int32(0), 0.0)
 
 mutable struct B200Simulation
     sim::Any
@@ -64,7 +70,8 @@ end
 """
     B200Simulation(sim, t_span; form = :fp32, device = 0, tiles = nothing, fft_schedules = Dict())
 
-A GPU twin of `sim` (laterally-variable ELVA with Maxwell mantle) over `t_span`, the
+A GPU twin of `sim` over `t_span` (form :fp32 runs the laterally-variable ELVA path;
+:fp64 also the ELRA, rigid-mantle and laterally-constant Maxwell rheologies), the
 same tuple given to `Simulation`: the same inputs, run by libfastiso_b200.so.  `tiles =
 (h_rows, B_cols)` and `fft_schedules = Dict(L => [radices...])` pass tuned settings
 (fastiso_b200's `tuning/b200.json`) to fi_set_tiles / fi_set_fft_schedule.
@@ -78,7 +85,23 @@ function B200Simulation(sim, t_span; form = :fp32, device = 0, tiles = nothing, 
     cfg.rho_ice, cfg.rho_water, cfg.rho_seawater = c.rho_ice, c.rho_water, c.rho_seawater
     cfg.rho_litho, cfg.rho_uppermantle = se.rho_litho, se.rho_uppermantle
     cfg.litho_poissonratio = se.litho_poissonratio
-    cfg.lithosphere = se.lithosphere isa RigidLithosphere ? Int32(1) : Int32(0)
+    cfg.lithosphere = se.lithosphere isa RigidLithosphere ? Int32(1) :
+                      se.lithosphere isa LaterallyConstantLithosphere ? Int32(2) : Int32(0)
+    cfg.mantle = se.mantle isa RelaxedMantle ? Int32(1) : se.mantle isa RigidMantle ? Int32(2) : Int32(0)
+    dq = sim.opts.diffeq
+    cfg.alg = dq.dt_min isa Real ? Int32(1) : Int32(0)          # Euler with dt_min, else BS3
+    cfg.dt_min = dq.dt_min isa Real ? Float64(dq.dt_min) : 0.0
+    cfg.sealevel_load = sl.load isa InteractiveSealevelLoad ? Int32(1) : Int32(0)
+    cfg.bsl_mode = sl.bsl isa ConstantOceanSurfaceBSL ? Int32(1) : sl.bsl isa PiecewiseConstantBSL ? Int32(2) :
+                   sl.bsl isa ImposedBSL ? Int32(3) : Int32(0)
+    cfg.bsl_update = sl.update_bsl isa ExternalBSLUpdate ? Int32(1) : Int32(0)
+    cfg.volume_contribution = sl.volume_contribution isa FastIsostasy.NoVolumeContribution ? Int32(0) : Int32(1)
+    cfg.density_contribution = sl.density_contribution isa FastIsostasy.NoDensityContribution ? Int32(0) : Int32(1)
+    cfg.adjustment_contribution = sl.adjustment_contribution isa FastIsostasy.GoelzerAdjustmentContribution ?
+                                  Int32(1) : Int32(0)
+    sl.bsl isa CombinedBSL && error("CombinedBSL is not supported")
+    cfg.z_bsl = Float64(sl.bsl.ref.z)
+    cfg.bsl_ref_A = Float64(sl.bsl.ref.A)
     cfg.lithosphere_column = se.lithosphere_column isa CompressibleLithosphereColumn ? Int32(1) : Int32(0)
     cfg.sea_surface = sl.surface isa LaterallyVariableSeaSurface ? Int32(1) : Int32(0)
     cfg.bc_viscous_border = bcs.viscous_displacement.x_border
@@ -110,6 +133,17 @@ function B200Simulation(sim, t_span; form = :fp32, device = 0, tiles = nothing, 
     set_field!(b, F.u_ref, sim.ref.u)
     set_field!(b, F.ue_ref, sim.ref.ue)
     set_field!(b, F.z_b_ref, sim.ref.z_b)
+    set_field!(b, F.tau, se.tau)
+    if sl.bsl isa PiecewiseConstantBSL
+        z = Vector{Float64}(sl.bsl.ref.z_vec)
+        A = Vector{Float64}([FastIsostasy.interpolate(zz, sl.bsl.ref.A_itp) for zz in z])
+        check(ccall((:fi_set_ocean_surface_table, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}),
+                    b.h, length(z), z, A), b.h, "fi_set_ocean_surface_table")
+    elseif sl.bsl isa ImposedBSL
+        t, z = Vector{Float64}(sl.bsl.t_vec), Vector{Float64}(sl.bsl.z_vec)
+        check(ccall((:fi_set_bsl_history, LIB), Cint, (Ptr{Cvoid}, Int32, Ptr{Float64}, Ptr{Float64}),
+                    b.h, length(t), t, z), b.h, "fi_set_bsl_history")
+    end
     if timeinterp
         t = Vector{Float64}(it.t_vec)
         H = cat((Array{Float64}(X) for X in it.H_vec)...; dims = 3)

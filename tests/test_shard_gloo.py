@@ -50,3 +50,22 @@ def test_two_gloo_ranks_gather(tmp_path):
     got = sorted(i for part in views[0] for i in part["members"])
     assert got == list(range(len(sizes)))
     assert [p["rank"] for p in views[0]] == [0, 1]
+
+
+def test_stiffness_weighted_partition():
+    import numpy as np
+
+    """Stiffer members (lower minimum viscosity) cost more; the partition balances the
+    weighted cost and the weighted greedy bound holds."""
+    from fastiso_b200.shard import stiffness_rate
+
+    D = 6.6e10 * 100e3**3 / (12 * (1 - 0.28**2))
+    assert stiffness_rate(1e19, D, 30e3) > 100 * stiffness_rate(1e21, D, 30e3) * 0.99
+    rng = np.random.default_rng(3)
+    sizes = list(rng.choice([64, 96, 128, 192, 256], size=40))
+    rates = list(10.0 ** rng.uniform(-1.0, 1.0, size=40))
+    for world in (1, 2, 3, 8):
+        parts = shard_members(sizes, world, rates)
+        assert sorted(i for p in parts for i in p) == list(range(40))
+        loads = [sum(member_cost(sizes[i], rates[i]) for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(member_cost(n, r) for n, r in zip(sizes, rates)) + 1e-6

@@ -228,13 +228,6 @@ static int get_plan(fi_handle* h, int L, int* out) {
     return FI_OK;
 }
 
-// FP32 transforms with a two-level decomposition (fi_fft.cuh) take it unless the
-// environment variable FI_FFT_TWO_LEVEL=0 selects the Stockham passes of the radix schedule.
-static bool two_level_enabled() {
-    const char* e = getenv("FI_FFT_TWO_LEVEL");
-    return !(e && e[0] == '0');
-}
-
 static int upload_plans(fi_handle* h) {
     std::vector<FftPlan> v(h->plans.size());
     for (size_t i = 0; i < v.size(); i++) {
@@ -245,7 +238,6 @@ static int upload_plans(fi_handle* h) {
         memcpy(v[i].mag_ns, h->plans[i].mag_ns, sizeof(v[i].mag_ns));
         v[i].tw32 = h->plans[i].tw32;
         v[i].tw64 = h->plans[i].tw64;
-        v[i].tl = two_level_enabled() ? two_level_code(v[i].L) : 0;
     }
     if (!h->d_plans || h->n_plans_dev != v.size()) {
         RET(dalloc(h, &h->d_plans, v.size()));
@@ -442,7 +434,6 @@ static int create_buffers(fi_handle* h) {
             memcpy(dst.mag_ns, q.mag_ns, sizeof(dst.mag_ns));
             dst.tw32 = q.tw32;
             dst.tw64 = q.tw64;
-            dst.tl = two_level_enabled() ? two_level_code(q.L) : 0;
         };
         cp(m.px, h->plan_x);
         cp(m.py, h->plan_y);

@@ -36,8 +36,6 @@ constexpr int FFT_MAX_LEN = 4096;
 struct FftPlan {
     int L;
     int npass;
-    int tl;      // two-level decomposition of the FP32 transforms (two_level_code), 0: Stockham passes
-    int pad_tl;
     int radix[FFT_MAX_PASSES];
     unsigned int mag_nb[FFT_MAX_PASSES];
     unsigned int mag_ns[FFT_MAX_PASSES];
@@ -238,151 +236,11 @@ __device__ __forceinline__ void stockham_pass_generic(const cplx<T>* __restrict_
     }
 }
 
-// ---------------------------------------------------------------------------
-// Two-level (four-step) transforms of the FP32 form: L = L1 L2 with L1, L2 <= 32.
-// One warp owns a transform.  Stage A: lane j2 < L2 loads x[j2 + L2 j1] (j1 < L1),
-// runs the length-L1 DFT in registers, multiplies by w_L^(j2 k1) and stores row k1 of
-// a rotated L1 x L2 scratch; stage B: lane k1 < L1 loads that row, runs the length-L2
-// DFT in registers and stores X[k1 + L1 k2].  The stages exchange through shared memory
-// with __syncwarp: two memory round trips and no block barrier per transform, where the
-// Stockham passes take one block barrier each.  The register DFTs are a composition
-// R1 x R2 of the SmallDft butterflies, every index known at compile time.
-// ---------------------------------------------------------------------------
-// code of the decomposition of L (host and device); 0 when L has none here
-__host__ __device__ inline int two_level_code(int L) {
-    switch (L) {
-        case 64: return 1;     // 8 x 8
-        case 96: return 2;     // 8 x 12
-        case 128: return 3;    // 8 x 16
-        case 192: return 4;    // 12 x 16
-        case 256: return 5;    // 16 x 16
-        case 350: return 6;    // 14 x 25
-        case 384: return 7;    // 16 x 24
-        case 512: return 8;    // 16 x 32
-        case 700: return 9;    // 28 x 25
-        case 1024: return 10;  // 32 x 32
-        default: return 0;
-    }
-}
-
-// length R1 R2 DFT of v (natural order in and out) in registers; the twiddles
-// w_N^m = tw[m * tstride] (tw: the length-L table, tstride = L / N)
-template <int R1, int R2, bool INV>
-__device__ __forceinline__ void reg_dft(float2* v, const float2* __restrict__ tw, int tstride) {
-    if constexpr (R2 == 1) {
-        SmallDft<R1, INV, float>::run(v);
-    } else {
-        constexpr int N = R1 * R2;
-        float2 a[N];
-#pragma unroll
-        for (int j2 = 0; j2 < R2; j2++) {
-            float2 t[R1];
-#pragma unroll
-            for (int j1 = 0; j1 < R1; j1++) t[j1] = v[j2 + R2 * j1];
-            SmallDft<R1, INV, float>::run(t);
-#pragma unroll
-            for (int k1 = 0; k1 < R1; k1++) {
-                if (j2 * k1 == 0) {
-                    a[k1 * R2 + j2] = t[k1];
-                } else {
-                    float2 w = tw[(j2 * k1) * tstride];
-                    if (INV) w.y = -w.y;
-                    a[k1 * R2 + j2] = cmul(t[k1], w);
-                }
-            }
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < R1; k1++) {
-            float2 t[R2];
-#pragma unroll
-            for (int j2 = 0; j2 < R2; j2++) t[j2] = a[k1 * R2 + j2];
-            SmallDft<R2, INV, float>::run(t);
-#pragma unroll
-            for (int k2 = 0; k2 < R2; k2++) v[k1 + R1 * k2] = t[k2];
-        }
-    }
-}
-
-template <int A1, int A2, int B1, int B2, bool INV>
-__device__ __noinline__ void fft_two_level(float2* __restrict__ x, float2* __restrict__ t,
-                                           const float2* __restrict__ tw, int nbatch, int bstride) {
-    constexpr int L1 = A1 * A2, L2 = B1 * B2, L = L1 * L2;
-    static_assert(L1 <= 32 && L2 <= 32, "one lane per sub-transform");
-    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int b = threadIdx.x >> 5; b < nbatch; b += nw) {
-        float2* xb = x + (size_t)b * bstride;
-        float2* tb = t + (size_t)b * bstride;
-        if (lane < L2) {
-            const int j2 = lane;
-            float2 v[L1];
-#pragma unroll
-            for (int j1 = 0; j1 < L1; j1++) v[j1] = xb[j2 + L2 * j1];
-            reg_dft<A1, A2, INV>(v, tw, L / L1);
-#pragma unroll
-            for (int k1 = 0; k1 < L1; k1++) {
-                float2 y = v[k1];
-                if (k1 > 0) {
-                    float2 w = tw[j2 * k1];
-                    if (INV) w.y = -w.y;
-                    y = cmul(y, w);
-                }
-                // row k1 rotated by k1: stage B's column reads hit distinct banks
-                int c = j2 + (k1 % L2);
-                c = c >= L2 ? c - L2 : c;
-                tb[k1 * L2 + c] = y;
-            }
-        }
-        __syncwarp();
-        if (lane < L1) {
-            const int k1 = lane;
-            float2 v[L2];
-#pragma unroll
-            for (int j2 = 0; j2 < L2; j2++) {
-                int c = j2 + (k1 % L2);
-                c = c >= L2 ? c - L2 : c;
-                v[j2] = tb[k1 * L2 + c];
-            }
-            reg_dft<B1, B2, INV>(v, tw, L / L2);
-#pragma unroll
-            for (int k2 = 0; k2 < L2; k2++) xb[k1 + L1 * k2] = v[k2];
-        }
-        __syncwarp();
-    }
-}
-
-// FP32 transforms of plan p with a two-level decomposition: result in buf0 (buf1 is the
-// scratch).  Returns false when p has none.
-template <bool INV>
-__device__ __noinline__ bool fft_two_level_dispatch(float2* buf0, float2* buf1, const FftPlan& p, int nbatch,
-                                                    int bstride) {
-    const float2* tw = p.tw32;
-    switch (p.tl) {
-        case 1: fft_two_level<8, 1, 8, 1, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 2: fft_two_level<8, 1, 3, 4, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 3: fft_two_level<8, 1, 4, 4, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 4: fft_two_level<3, 4, 4, 4, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 5: fft_two_level<4, 4, 4, 4, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 6: fft_two_level<2, 7, 5, 5, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 7: fft_two_level<4, 4, 3, 8, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 8: fft_two_level<4, 4, 4, 8, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 9: fft_two_level<4, 7, 5, 5, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        case 10: fft_two_level<4, 8, 4, 8, INV>(buf0, buf1, tw, nbatch, bstride); return true;
-        default: return false;
-    }
-}
-
 // Runs all passes of plan p on buf0 (scratch buf1), returns where the result is.
 // Every thread of the block must call it (it synchronises between passes).
 template <bool INV, typename T>
 __device__ cplx<T>* fft_batch(cplx<T>* buf0, cplx<T>* buf1, const FftPlan& p, int nbatch, int bstride) {
     using C = cplx<T>;
-    if constexpr (sizeof(T) == sizeof(float)) {
-        if (p.tl) {
-            fft_two_level_dispatch<INV>(buf0, buf1, p, nbatch, bstride);
-            __syncthreads();
-            return buf0;
-        }
-    }
     const C* tw = plan_tw<T>(p);
     const int tid = threadIdx.x, nth = blockDim.x;
     C* src = buf0;

@@ -38,6 +38,7 @@ struct Plan {
     int npass;
     int radix[FFT_MAX_PASSES];
     unsigned mag_nb[FFT_MAX_PASSES], mag_ns[FFT_MAX_PASSES];
+    int nb[FFT_MAX_PASSES], tstride[FFT_MAX_PASSES], ns[FFT_MAX_PASSES];
     float2* tw32;
     double2* tw64;
 };
@@ -185,6 +186,9 @@ static void plan_schedule(Plan& p, const int* radix, int np) {
         p.radix[i] = radix[i];
         p.mag_nb[i] = fastdiv_magic((unsigned)(p.L / radix[i]));
         p.mag_ns[i] = fastdiv_magic((unsigned)Ns);
+        p.nb[i] = p.L / radix[i];
+        p.tstride[i] = p.L / (Ns * radix[i]);
+        p.ns[i] = Ns;
         Ns *= radix[i];
     }
 }
@@ -228,6 +232,29 @@ static int get_plan(fi_handle* h, int L, int* out) {
     return FI_OK;
 }
 
+static void copy_plan(const Plan& q, FftPlan& dst) {
+    dst.L = q.L;
+    dst.npass = q.npass;
+    memcpy(dst.radix, q.radix, sizeof(dst.radix));
+    memcpy(dst.mag_nb, q.mag_nb, sizeof(dst.mag_nb));
+    memcpy(dst.mag_ns, q.mag_ns, sizeof(dst.mag_ns));
+    memcpy(dst.nb, q.nb, sizeof(dst.nb));
+    memcpy(dst.tstride, q.tstride, sizeof(dst.tstride));
+    memcpy(dst.ns, q.ns, sizeof(dst.ns));
+    dst.tw32 = q.tw32;
+    dst.tw64 = q.tw64;
+}
+
+// The FP32 kernels read the plans from the member descriptor (staged in shared memory);
+// refreshed whenever a schedule changes before fi_init uploads the descriptor.
+static void copy_member_plans(fi_handle* h) {
+    Member& m = h->mem;
+    copy_plan(h->plans[h->plan_x], m.px);
+    copy_plan(h->plans[h->plan_y], m.py);
+    copy_plan(h->plans[h->plan_Mx], m.pMx);
+    copy_plan(h->plans[h->plan_My], m.pMy);
+}
+
 static int upload_plans(fi_handle* h) {
     std::vector<FftPlan> v(h->plans.size());
     for (size_t i = 0; i < v.size(); i++) {
@@ -236,6 +263,9 @@ static int upload_plans(fi_handle* h) {
         memcpy(v[i].radix, h->plans[i].radix, sizeof(v[i].radix));
         memcpy(v[i].mag_nb, h->plans[i].mag_nb, sizeof(v[i].mag_nb));
         memcpy(v[i].mag_ns, h->plans[i].mag_ns, sizeof(v[i].mag_ns));
+        memcpy(v[i].nb, h->plans[i].nb, sizeof(v[i].nb));
+        memcpy(v[i].tstride, h->plans[i].tstride, sizeof(v[i].tstride));
+        memcpy(v[i].ns, h->plans[i].ns, sizeof(v[i].ns));
         v[i].tw32 = h->plans[i].tw32;
         v[i].tw64 = h->plans[i].tw64;
     }
@@ -425,20 +455,7 @@ static int create_buffers(fi_handle* h) {
         m.Mx = h->Mx; m.My = h->My; m.MH = h->MH; m.msp = h->msp;
         m.i1 = h->i1; m.j1 = h->j1;
         m.plan_x = h->plan_x; m.plan_y = h->plan_y; m.plan_Mx = h->plan_Mx; m.plan_My = h->plan_My;
-        auto cp = [&](FftPlan& dst, int idx) {
-            const Plan& q = h->plans[idx];
-            dst.L = q.L;
-            dst.npass = q.npass;
-            memcpy(dst.radix, q.radix, sizeof(dst.radix));
-            memcpy(dst.mag_nb, q.mag_nb, sizeof(dst.mag_nb));
-            memcpy(dst.mag_ns, q.mag_ns, sizeof(dst.mag_ns));
-            dst.tw32 = q.tw32;
-            dst.tw64 = q.tw64;
-        };
-        cp(m.px, h->plan_x);
-        cp(m.py, h->plan_y);
-        cp(m.pMx, h->plan_Mx);
-        cp(m.pMy, h->plan_My);
+        copy_member_plans(h);
         for (int b = 0; b < 2; b++) {
             RET(dalloc(h, &m.u[b], n));
             RET(dalloc(h, &m.k14[b], n));
@@ -755,6 +772,7 @@ extern "C" int fi_set_fft_schedule(fi_handle* h, int32_t L, int32_t n, const int
     if (prod != L) return set_err(h, FI_ERR_ARG, "radices do not multiply to %d", L);
     plan_schedule(h->plans[it->second], radix, n);
     RET(upload_plans(h));
+    if (h->cfg.form == FI_FORM_FP32) copy_member_plans(h);
     CK(cudaStreamSynchronize(h->stream));
     return FI_OK;
 }

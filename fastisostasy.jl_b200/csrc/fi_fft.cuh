@@ -39,6 +39,11 @@ struct FftPlan {
     int radix[FFT_MAX_PASSES];
     unsigned int mag_nb[FFT_MAX_PASSES];
     unsigned int mag_ns[FFT_MAX_PASSES];
+    // per pass: L / R, the twiddle stride L / (Ns R) and Ns (product of the earlier
+    // radices), precomputed so that no pass divides by a runtime value
+    int nb[FFT_MAX_PASSES];
+    int tstride[FFT_MAX_PASSES];
+    int ns[FFT_MAX_PASSES];
     const float2* tw32;
     const double2* tw64;
 };
@@ -175,11 +180,10 @@ template <bool INV, typename T> struct SmallDft<8, INV, T> {
 // ---------------------------------------------------------------------------
 template <int R, bool INV, typename T>
 __device__ __forceinline__ void stockham_pass(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst,
-                                              const cplx<T>* __restrict__ tw, int L, int Ns, int nbatch,
-                                              int bstride, int tid, int nth, unsigned int mnb, unsigned int mns) {
+                                              const cplx<T>* __restrict__ tw, int nb, int stride, int Ns,
+                                              int nbatch, int bstride, int tid, int nth, unsigned int mnb,
+                                              unsigned int mns) {
     using C = cplx<T>;
-    const int nb = L / R;
-    const int stride = L / (Ns * R);
     const int total = nbatch * nb;
     for (int idx = tid; idx < total; idx += nth) {
         const int b = (int)fastdiv((unsigned)idx, (unsigned)nb, mnb);
@@ -245,24 +249,22 @@ __device__ cplx<T>* fft_batch(cplx<T>* buf0, cplx<T>* buf1, const FftPlan& p, in
     const int tid = threadIdx.x, nth = blockDim.x;
     C* src = buf0;
     C* dst = buf1;
-    int Ns = 1;
     for (int ps = 0; ps < p.npass; ps++) {
-        const int R = p.radix[ps];
+        const int R = p.radix[ps], nb = p.nb[ps], ts = p.tstride[ps], Ns = p.ns[ps];
         const unsigned mnb = p.mag_nb[ps], mns = p.mag_ns[ps];
         switch (R) {
-            case 2: stockham_pass<2, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
-            case 3: stockham_pass<3, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
-            case 4: stockham_pass<4, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
-            case 5: stockham_pass<5, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
-            case 7: stockham_pass<7, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
-            case 8: stockham_pass<8, INV, T>(src, dst, tw, p.L, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 2: stockham_pass<2, INV, T>(src, dst, tw, nb, ts, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 3: stockham_pass<3, INV, T>(src, dst, tw, nb, ts, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 4: stockham_pass<4, INV, T>(src, dst, tw, nb, ts, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 5: stockham_pass<5, INV, T>(src, dst, tw, nb, ts, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 7: stockham_pass<7, INV, T>(src, dst, tw, nb, ts, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
+            case 8: stockham_pass<8, INV, T>(src, dst, tw, nb, ts, Ns, nbatch, bstride, tid, nth, mnb, mns); break;
             default: stockham_pass_generic<INV, T>(src, dst, tw, p.L, R, Ns, nbatch, bstride, tid, nth); break;
         }
         __syncthreads();
         C* t = src;
         src = dst;
         dst = t;
-        Ns *= R;
     }
     return src;
 }

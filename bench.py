@@ -352,6 +352,45 @@ def output_bench(dev, kyr=2.0, every=100.0):
     return res
 
 
+def config2_full(dev, kyr=120.0, seg=10.0):
+    """The whole N = 350 glacial cycle (120 kyr): the plain FP64 form's adaptive run
+    (recorded), the FP32 form's adaptive run, and the FP32 form replaying the FP64 record;
+    kyr/s of each and rel-L2 of u and dz_ss at every `seg`-kyr output (FP32 replay vs
+    FP64, FP32 adaptive vs FP64)."""
+    outs = [float(t) for t in np.arange(seg, kyr + 1e-9, seg) * 1e3]
+
+    def run(form, record=False, replay=None):
+        sim = W.config2(form=form, N=N350, t_end=kyr * 1e3)
+        sim.cfg.device = dev
+        sim.cfg.max_steps = 500_000_000
+        sim.nout.t = outs
+        integ = F.init_integrator(sim)
+        if record:
+            sim.record_steps(1 << 26)
+        if replay is not None:
+            sim.set_step_replay(replay)
+        fields, ms = [], 0.0
+        for t in outs:
+            F.step(integ, t - integ.t, True)
+            ms += sim.stats()["last_gpu_ms"]
+            fields.append({f: sim.get_field(f) for f in ("u", "dz_ss")})
+        st = sim.stats()
+        rec = sim.step_record() if record else None
+        sim.close()
+        return fields, ms, st, rec
+
+    f64, ms64, st64, rec = run("fp64", record=True)
+    f32, ms32, st32, _ = run("fp32")
+    fr, msr, _, _ = run("fp32", replay=rec)
+    err = lambda a, b, f: [rel_l2(x[f], y[f]) for x, y in zip(a, b)]  # noqa: E731
+    return {"kyr": kyr, "fp64": {"kyr_per_s": kyr / (ms64 / 1e3), "attempts": st64["naccept"] + st64["nreject"]},
+            "fp32": {"kyr_per_s": kyr / (ms32 / 1e3), "attempts": st32["naccept"] + st32["nreject"]},
+            "speedup": ms64 / ms32,
+            "fp32_replay_vs_fp64": {"u": err(fr, f64, "u"), "dz_ss": err(fr, f64, "dz_ss")},
+            "fp32_adaptive_vs_fp64": {"u": err(f32, f64, "u"), "dz_ss": err(f32, f64, "dz_ss")},
+            "outputs_kyr": [t / 1e3 for t in outs]}
+
+
 def fno_flops_per_sample(S=128, C=32, KX=16, KY=32, PW=128, nin=6, layers=4):
     """Algorithmic FLOPs of one forward pass of the surrogate per sample (the GEMMs as
     contracted, without padding): lift, per layer the DFT along x and y, the mode mixing,
@@ -709,6 +748,8 @@ def main():
                     help="N=1024: 5 yr warm-up launch, then one 0.2-yr launch of k_persist (ncu capture target)")
     ap.add_argument("--config5", action="store_true",
                     help="only the N=1024 high-resolution case (short window, roofline, rel-L2 vs FP64)")
+    ap.add_argument("--config2-full", action="store_true",
+                    help="the whole 120-kyr N=350 cycle: plain FP64 (recorded), FP32 adaptive, FP32 replay")
     ap.add_argument("--outputs", action="store_true",
                     help="only the output-pipeline leg (run! with outputs every 100 yr vs one output)")
     args = ap.parse_args()
@@ -742,6 +783,9 @@ def main():
         return
     if args.config5:
         print(json.dumps({"config5": config5_bench(local)}), flush=True)
+        return
+    if args.config2_full:
+        print(json.dumps({"config2_full": config2_full(local)}), flush=True)
         return
     if args.outputs:
         print(json.dumps({"output_pipeline": output_bench(local)}), flush=True)

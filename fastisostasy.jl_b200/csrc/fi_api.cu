@@ -117,7 +117,8 @@ struct fi_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double gpu_ms = 0.0, last_gpu_ms = 0.0;
     long long segments = 0;
-    size_t smem_cap = 0;
+    size_t smem_cap = 0;    // dynamic shared memory every per-phase kernel accepts
+    size_t smem_optin = 0;  // the device's opt-in shared memory per block
     double last_rhs_t = 0.0;
     long long nf_plain = 0;
     // asynchronous output pipeline of fi_run: two staging slots (device FP64 copies of
@@ -523,14 +524,24 @@ static int create_buffers(fi_handle* h) {
         RET(mk(&h->t_crow, h->ny));
         RET(mk(&h->t_ccol, h->MH));
         RET(mk(&h->t_crowi, h->ny + 2));
-        // opt in to the full shared memory per block; the actual need (which depends on the
-        // ice-table length) is checked in fi_init
+        // opt in to the full shared memory per block less each kernel's static shared
+        // memory (member descriptor, control block, plans); the actual need (which
+        // depends on the ice-table length) is checked in fi_init
         int smax = 0;
         CK(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->cfg.device));
+        h->smem_optin = (size_t)smax;
         const void* fk[] = {(const void*)k_rows_fwd, (const void*)k_cols, (const void*)k_rows_inv,
                             (const void*)k_conv_rows, (const void*)k_conv_cols, (const void*)k_conv_rows_inv};
-        for (const void* f : fk) CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smax - 4096));
-        h->smem_cap = (size_t)(smax - 4096);
+        size_t cap = (size_t)smax;
+        for (const void* f : fk) {
+            cudaFuncAttributes fa{};
+            CK(cudaFuncGetAttributes(&fa, f));
+            if (fa.sharedSizeBytes >= (size_t)smax) return set_err(h, FI_ERR_CUDA, "static shared memory too large");
+            const size_t dyn = (size_t)smax - fa.sharedSizeBytes;
+            CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            cap = std::min(cap, dyn);
+        }
+        h->smem_cap = cap;
     } else {
         PlainBufs& p = h->p;
         const size_t M = (size_t)h->Mx * h->My;
@@ -1339,7 +1350,7 @@ static int rhs_plain(fi_handle* h, double t, double* u, double* dudt) {
         CKL();
         return FI_OK;
     }
-    if (c.lithosphere != FI_LITHO_LATERALLY_VARIABLE) {
+    if (c.lithosphere == FI_LITHO_LATERALLY_CONSTANT) {
         // one step of dt_min written into u in place; dudt is left as it is
         kp_lc_in<<<g, NT, 0, h->stream>>>(p.s_load, p.s_l, c.g, u, p.fftrhs, p.fftU, n);
         CKL();
@@ -1628,7 +1639,7 @@ static int plan_layouts(fi_handle* h, int K) {
                            rows_inv_smem(h->nx, h->h_rows, h->n_cols), conv_rows_smem(h->Mx, h->h_conv),
                            conv_cols_smem(h->My, h->B_conv)};
     for (size_t q : need)
-        if (q + sizeof(fi::Member) + sizeof(fi::Ctl) + 4096 > h->smem_cap)
+        if (q + 1024 > h->smem_cap)
             return set_err(h, FI_ERR_ARG, "shared memory need %zu B exceeds the per-block limit", q);
     return setup_persist(h, K);
 }
@@ -1650,7 +1661,10 @@ static int setup_persist(fi_handle* h, int K) {
     int coop = 0, nsm = 0, occ = 0;
     CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->cfg.device));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->cfg.device));
-    if (!coop || smem + 8192 > h->smem_cap) {
+    cudaFuncAttributes fp{}, fp1{};
+    CK(cudaFuncGetAttributes(&fp, k_persist));
+    CK(cudaFuncGetAttributes(&fp1, k_persist1));
+    if (!coop || smem + std::max(fp.sharedSizeBytes, fp1.sharedSizeBytes) + 1024 > h->smem_optin) {
         h->executor = EXEC_GRAPH;
         return FI_OK;
     }
@@ -1799,8 +1813,12 @@ static int reeval_fsal(fi_handle* h) {
         RET(rhs_fused(h, 1, nullptr, nullptr, nullptr));
         RET(read_ctl(h));
     } else {
-        // uprev <- u (same values); f(fsalfirst, u, p, t)
-        RET(rhs_plain(h, h->ctl.t, h->p.u[h->ctl.ibuf], h->p.k14[h->ctl.ik]));
+        // apply_step!: uprev <- u, then f(fsalfirst, u, p, t) on the integrator's u, whose
+        // in-place changes (the laterally constant Maxwell step writes u) the next
+        // perform_step! overwrites from uprev: evaluate on a copy so that uprev stays
+        const size_t n = N2(h);
+        CK(cudaMemcpyAsync(h->p.tmp, h->p.u[h->ctl.ibuf], n * 8, cudaMemcpyDeviceToDevice, h->stream));
+        RET(rhs_plain(h, h->ctl.t, h->p.tmp, h->p.k14[h->ctl.ik]));
     }
     return FI_OK;
 }

@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(256) k_act_bwd(const float* __restrict__ dv, c
 // accumulates sum(dq) (gradient of b2).
 __global__ void __launch_bounds__(256) k_loss(const float* __restrict__ q, const float* __restrict__ target,
                                               const float* __restrict__ w, const float* __restrict__ dy, int n,
-                                              int S2, float inv_n, float* dq, bf16* vext4, float* loss, float* gb2) {
+                                              int S2, float inv_n, float* dq, bf16* vext4, float* part) {
     const int i = blockIdx.x * 256 + threadIdx.x;
     float l = 0.f, d = 0.f;
     if (i < n) {
@@ -367,8 +367,32 @@ __global__ void __launch_bounds__(256) k_loss(const float* __restrict__ q, const
             a += sl[w];
             c += sd[w];
         }
-        atomicAdd(loss, a);
-        atomicAdd(gb2, c);
+        part[blockIdx.x] = a;
+        part[gridDim.x + blockIdx.x] = c;
+    }
+}
+
+// the per-block partials of k_loss summed in a fixed order (one block): the loss and the
+// output-bias gradient come out the same on every run
+__global__ void __launch_bounds__(256) k_loss_sum(const float* __restrict__ part, int nblk, float* loss, float* gb2) {
+    __shared__ float sl[256], sd[256];
+    float a = 0.f, c = 0.f;
+    for (int i = threadIdx.x; i < nblk; i += 256) {
+        a += part[i];
+        c += part[nblk + i];
+    }
+    sl[threadIdx.x] = a;
+    sd[threadIdx.x] = c;
+    for (int o = 128; o > 0; o >>= 1) {
+        __syncthreads();
+        if (threadIdx.x < o) {
+            sl[threadIdx.x] += sl[threadIdx.x + o];
+            sd[threadIdx.x] += sd[threadIdx.x + o];
+        }
+    }
+    if (threadIdx.x == 0) {
+        *loss = sl[0];
+        *gb2 += sd[0];
     }
 }
 
@@ -408,18 +432,39 @@ __global__ void __launch_bounds__(256) k_spec_wgrad(const bf16* __restrict__ Z, 
 }
 
 // split-K partials [z][MN] summed over z and added to grad[base + map[i]] (map < 0: not a
-// parameter; grad is zeroed before the backward pass).  Block (x, y) sums the z range y of
-// gridDim.y for 256 consecutive i.
-__global__ void k_reduce_map(const float* __restrict__ part, int nz, int MN, const int* __restrict__ map,
-                             float* grad, long long base) {
+// parameter; grad is zeroed before the backward pass; map is one-to-one), in two passes
+// with a fixed summation order, so that gradients are the same on every run.  Pass 1:
+// block (x, y) sums the z range y of gridDim.y for 256 consecutive i and leaves the sum
+// in row z0 of its own range.  Pass 2 (k_reduce_map_fin) adds the ranges in order.
+__global__ void k_reduce_map(float* part, int nz, int MN, const int* __restrict__ map) {
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= MN) return;
+    if (map[i] < 0) return;
+    const int per = (nz + gridDim.y - 1) / gridDim.y, z0 = blockIdx.y * per, z1 = min(nz, z0 + per);
+    if (z1 <= z0) return;
+    float s = 0.f;
+    for (int z = z0; z < z1; z++) s += part[(size_t)z * MN + i];
+    part[(size_t)z0 * MN + i] = s;
+}
+
+__global__ void k_reduce_map_fin(const float* __restrict__ part, int nz, int MN, int ny,
+                                 const int* __restrict__ map, float* grad, long long base) {
     const int i = blockIdx.x * 256 + threadIdx.x;
     if (i >= MN) return;
     const int t = map[i];
     if (t < 0) return;
-    const int per = (nz + gridDim.y - 1) / gridDim.y, z0 = blockIdx.y * per, z1 = min(nz, z0 + per);
+    const int per = (nz + ny - 1) / ny;
     float s = 0.f;
-    for (int z = z0; z < z1; z++) s += part[(size_t)z * MN + i];
-    if (z1 > z0) atomicAdd(&grad[base + t], s);
+    for (int z0 = 0; z0 < nz; z0 += per) s += part[(size_t)z0 * MN + i];
+    grad[base + t] += s;
+}
+
+static cudaError_t reduce_map(float* part, cudaStream_t st, int nz, int MN, int ny, const int* map, float* grad,
+                              long long base) {
+    const unsigned gx = (unsigned)((MN + 255) / 256);
+    k_reduce_map<<<dim3(gx, ny), 256, 0, st>>>(part, nz, MN, map);
+    k_reduce_map_fin<<<gx, 256, 0, st>>>(part, nz, MN, ny, map, grad, base);
+    return cudaGetLastError();
 }
 
 __global__ void k_adam(float* p, const float* __restrict__ g, float* m, float* v, long long n, float lr, float b1,
@@ -712,9 +757,7 @@ int backward(fi_fno* h, int B) {
                 EpiProjBwd{h->params + o.b1, h->params + o.Q2, h->dq, h->da_rows, h->daT, S2}));
     FNO_CK(gemm(h, 2 * PW, VC, SL, opK(h->daT, S2, (long long)2 * PW * S2, SL), opK(v4, S2, vs, SL), B * ns,
                 EpiStoreF32{h->part, VC, (long long)2 * PW * VC}, ns));
-    k_reduce_map<<<dim3((2 * PW * VC + 255) / 256, 16), 256, 0, h->st>>>(h->part, B * ns, 2 * PW * VC, h->map_proj,
-                                                                        gr, 0);
-    FNO_CK(cudaGetLastError());
+    FNO_CK(reduce_map(h->part, h->st, B * ns, 2 * PW * VC, 16, h->map_proj, gr, 0));
     FNO_CK(gemm(h, B * S2, C, PW, opK(h->da_rows, PW), opK(h->Q1Tb, PW), 1, EpiNchw{h->dvf, S2, 0}));
     for (int l = NLAYER - 1; l >= 0; l--) {
         k_act_bwd<<<B * (S2 / 64), 256, 0, h->st>>>(h->dvf, l < NLAYER - 1 ? h->zs[l] : nullptr, h->dz, nullptr, S2);
@@ -722,9 +765,7 @@ int backward(fi_fno* h, int B) {
         // pointwise path weights and bias: [co][ci | ones]
         FNO_CK(gemm(h, C, C + 1, SL, opK(h->dz, S2, cs, SL), opK(h->vext[l], S2, vs, SL), B * ns,
                     EpiStoreF32{h->part, C + 1, (long long)C * (C + 1)}, ns));
-        k_reduce_map<<<dim3((C * (C + 1) + 255) / 256, 32), 256, 0, h->st>>>(h->part, B * ns, C * (C + 1),
-                                                                             h->map_loc, gr, o.layer[l]);
-        FNO_CK(cudaGetLastError());
+        FNO_CK(reduce_map(h->part, h->st, B * ns, C * (C + 1), 32, h->map_loc, gr, o.layer[l]));
         // spectral path: adjoint of the inverse DFT along x, then along y
         FNO_CK(gemm(h, B * C * S, 2 * KX, S, opK(h->dz, S), opK(h->G1T, S), 1, EpiDftX{h->Tb, B, S, 0}));
         FNO_CK(gemm(h, KX * B * C, 2 * KY, 2 * S, opK(h->Tb, 2 * S), opK(h->G2T, 2 * S), 1, EpiModes{h->dYm, B}));
@@ -744,8 +785,7 @@ int backward(fi_fno* h, int B) {
     FNO_CK(cudaGetLastError());
     FNO_CK(gemm(h, C, XC, SL, opK(h->dz, S2, cs, SL), opK(h->xe, S2, (long long)XC * S2, SL), B * ns,
                 EpiStoreF32{h->part, XC, (long long)C * XC}, ns));
-    k_reduce_map<<<dim3(1, 64), 256, 0, h->st>>>(h->part, B * ns, C * XC, h->map_lift, gr, 0);
-    FNO_CK(cudaGetLastError());
+    FNO_CK(reduce_map(h->part, h->st, B * ns, C * XC, 64, h->map_lift, gr, 0));
     return FI_OK;
 }
 
@@ -753,8 +793,10 @@ int set_loss(fi_fno* h, int B, const float* target, const float* w, const float*
     const int n = B * h->S2;
     FNO_CK(cudaMemsetAsync(h->grads, 0, sizeof(float) * h->o.total, h->st));
     FNO_CK(cudaMemsetAsync(h->scal, 0, sizeof(float) * 4, h->st));
-    k_loss<<<(n + 255) / 256, 256, 0, h->st>>>(h->q, target, w, dy, n, h->S2, 1.f / n, h->dq, h->vext[NLAYER],
-                                               h->scal, h->grads + h->o.b2);
+    // per-block partials in the split-K scratch (free until the backward pass)
+    const int nblk = (n + 255) / 256;
+    k_loss<<<nblk, 256, 0, h->st>>>(h->q, target, w, dy, n, h->S2, 1.f / n, h->dq, h->vext[NLAYER], h->part);
+    k_loss_sum<<<1, 256, 0, h->st>>>(h->part, nblk, h->scal, h->grads + h->o.b2);
     FNO_CK(cudaGetLastError());
     return FI_OK;
 }

@@ -933,11 +933,15 @@ static int rhs_impl(or_sim* s, double t, double* u, double* dudt) {
             if (!isfinite(dudt[k])) return set_err(s, FI_ERR_NONFINITE, "non-finite dudt");
         return FI_OK;
     }
-    if (c->lithosphere != FI_LITHO_LATERALLY_VARIABLE) {
-        /* MaxwellMantle with a laterally constant or rigid lithosphere (Bueler et al. 2007,
+    if (c->lithosphere == FI_LITHO_LATERALLY_CONSTANT) {
+        /* MaxwellMantle with a laterally constant lithosphere (Bueler et al. 2007,
          * src/deformation.jl:52-89): one step of dt_min of the spectral scheme
          * U+ = ((nabla - dt/2 beta) U + dt F) / (nabla + dt/2 beta), nabla = 2 eta |k| R,
-         * beta = rho_m g + D |k|^4, written into u in place; dudt is left as it is */
+         * beta = rho_m g + D |k|^4, written into u in place; dudt is left as it is.
+         * A rigid lithosphere keeps the laterally variable operator below with a zero
+         * elastic response: src/deformation.jl:15 lists MaxwellMantle with
+         * RigidLithosphere as not implemented, and the operator with u_e = 0 is the
+         * behaviour both forms of this library share for it. */
         const double dt = c->dt_min * c->seconds_per_year;
         for (size_t k = 0; k < n; k++) {
             s->fftrhs[k].re = -(s->c_load[k] + s->c_litho[k]) * c->g; /* K == 1 */

@@ -84,9 +84,6 @@ def lib_outputs(sim, t_outs, fields=("u", "dudt", "dz_ss"), record=0, replay=Non
     return out, (sim.step_record() if record else None)
 
 
-ORACLE_FIELD_IDS = {"u": 8, "dudt": 10, "dz_ss": 11, "ue": 9}
-
-
 def oracle_outputs(ref, t_outs, fields=("u", "dudt", "dz_ss"), record=0, replay=None):
     """The same for the oracle (already initialised with ref.init())."""
     ref.init_integrator(np.asarray(t_outs, dtype=np.float64))
@@ -98,7 +95,7 @@ def oracle_outputs(ref, t_outs, fields=("u", "dudt", "dz_ss"), record=0, replay=
     for t in t_outs:
         ref.step(t - ref.stats()["t"])
         for f in fields:
-            out[f].append(ref.get_field(ORACLE_FIELD_IDS[f]))
+            out[f].append(ref.get_field(abi.FIELDS[f]))
     return out, (ref.step_record() if record else None)
 
 

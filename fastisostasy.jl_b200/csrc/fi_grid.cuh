@@ -2,11 +2,15 @@
 // fi_ensemble.cu): the bounded grid barrier, the phase timeline marks and the step
 // controller run by one warp.
 //
-// The grid barrier is an arrival counter plus a generation word.  Each wait is
-// bounded: after PERSIST_SPIN_LIMIT polls the block raises the abort word and leaves,
-// every other block sees the abort word at its next poll and leaves too, and the
-// host reports FI_ERR_TIMEOUT.  A cooperative launch guarantees that all blocks are
-// resident, so the bound is only reached if the launch is broken.
+// The grid barrier is one 64-bit arrival counter that only grows (zeroed by the host
+// before each launch): a block adds 1 with acq_rel semantics and waits, polling with
+// acquire loads, until the counter reaches the next multiple of the block count, so
+// one atomic round trip and one load round trip are the whole critical path.  Each
+// wait is bounded: after PERSIST_SPIN_LIMIT polls the block raises the abort word
+// (bar[2]) and leaves, every other block sees the abort word at one of its next polls
+// and leaves too, and the host reports FI_ERR_TIMEOUT.  A cooperative launch
+// guarantees that all blocks are resident, so the bound is only reached if the launch
+// is broken (or a test asks for more arrivals than blocks).
 #pragma once
 #include "fi_phases.cuh"
 
@@ -14,34 +18,35 @@ namespace fi {
 
 
 // Returns false (in every thread of the block) when the barrier was abandoned.
-// polls: the wait bound (PERSIST_SPIN_LIMIT unless a test lowers it).
+// polls: the wait bound (PERSIST_SPIN_LIMIT unless a test lowers it).  bar: 16 bytes,
+// 8-byte aligned: [0..1] the arrival counter, [2] the abort word.
 __device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, int* s_ok,
                                              long long polls = PERSIST_SPIN_LIMIT) {
-    __syncthreads();
+    __syncthreads();  // the block's writes happen before thread 0's release
     if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = bar + 1;
-        volatile unsigned int* vabort = bar + 2;
-        const unsigned int gen = *vgen;
+        unsigned long long* cnt = reinterpret_cast<unsigned long long*>(bar);
+        const volatile unsigned int* vabort = bar + 2;
+        unsigned long long old, cur;
+        asm volatile("atom.add.acq_rel.gpu.u64 %0, [%1], 1;" : "=l"(old) : "l"(cnt) : "memory");
+        const unsigned long long target = (old / nblocks + 1) * nblocks;
         int ok = 1;
-        __threadfence();
-        const unsigned int prev = atomicAdd(bar, 1u);
-        if (prev == nblocks - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
+        if (old + 1 != target) {
             long long npoll = 0;
-            while (*vgen == gen) {
-                if (*vabort) { ok = 0; break; }
+            for (;;) {
+                asm volatile("ld.acquire.gpu.u64 %0, [%1];" : "=l"(cur) : "l"(cnt) : "memory");
+                if (cur >= target) break;
                 if (++npoll > polls) {
                     atomicExch(bar + 2, 1u);
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                if ((npoll & 63) == 0 && *vabort) {
+                    ok = 0;
+                    break;
+                }
+                if (npoll > 4096) __nanosleep(100);
             }
-        }
-        __threadfence();
+        }  // else: the last arrival, whose acq_rel atomic read every other block's release
         *s_ok = ok;
     }
     __syncthreads();

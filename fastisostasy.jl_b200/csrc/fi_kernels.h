@@ -53,8 +53,11 @@ enum {
     PH_ROWS_FWD2, PH_COLS2, PH_ROWS_FWD3, PH_COLS3, PH_ROWS_FWD4, PH_COLS4, PH_ROWS_INV4, PH_CONTROLLER,
     PH_COUNT
 };
-__global__ void k_persist(PersistArgs a);   // two blocks per SM
-__global__ void k_persist1(PersistArgs a);  // one block per SM (larger register budget)
+// The persistent step kernel whose row and column transforms run the compiled radix
+// sequences seqx / seqy (fi_fft.cuh seq_code), built for two blocks per SM (minb 2) or
+// one (minb 1, larger register budget); pairs without a compiled kernel get the one
+// that runs the plans' runtime passes.
+const void* persist_kernel(int seqx, int seqy, int minb);
 // fills the shared-memory layout fields of a and returns the dynamic shared memory bytes
 size_t persist_layout(int nx, int ny, int Mx, int My, int K, int fwd_bytes, int h_rows, int ncols, int B_cols,
                       int h_conv, int B_conv, PersistArgs* a);

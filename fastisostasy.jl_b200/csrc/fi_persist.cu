@@ -28,6 +28,9 @@ namespace fi {
 // The executor body, inlined into two kernels whose register budgets differ: k_persist
 // for two blocks per SM (64 registers a thread) where shared memory fits two blocks,
 // k_persist1 for one (no spills) where it fits only one.
+// SX / SY: the compiled radix sequences of the row and column transforms (0: the
+// plans' runtime passes).
+template <int SX, int SY>
 __device__ __forceinline__ void persist_body(const PersistArgs& a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Member sm;
@@ -135,7 +138,7 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
             if (tid == 0) fwd_offsets(m, sc, s_uc, fs);
             __syncthreads();
             while (t < a.n_rows) {
-                ph_rows_fwd(m, fs, fv, pl[0], smem, row_ranges(t, a.h_rows, ny), a.h_rows, Sout, inv, Sprev, kdst);
+                ph_rows_fwd<SX>(m, fs, fv, pl[0], smem, row_ranges(t, a.h_rows, ny), a.h_rows, Sout, inv, Sprev, kdst);
                 t += G;
                 if (t < a.n_rows) {
                     fwd_prefetch(m, fs, smem, row_ranges(t, a.h_rows, ny), inv, Sprev, &fv);
@@ -147,7 +150,7 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
             trace_mark(trace, &tlast, PH_ROWS_FWD2 + 2 * (stage - 2));
             // ---- columns; count the call and evaluate the gate of the next one ----
             for (int tc = bid; tc < a.n_cols; tc += G)
-                ph_cols(m, pl[1], pl[0].tw32, smem, tc, a.B_cols, Sout, m.cpart + 4 * tc);
+                ph_cols<SY>(m, pl[1], pl[0].tw32, smem, tc, a.B_cols, Sout, m.cpart + 4 * tc);
             if (tid == 0) {
                 sc.nf += 1;
                 if (stage < 4) gate_eval(m, &sc, sc.t + (stage == 2 ? C3 : 1.0) * sc.dt);
@@ -180,7 +183,7 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
             corners_from_partials((const double*)(smem + L.cpart), m.ncols, s_c4);
             __syncthreads();
             while (t < a.n_rows) {
-                const double sum = ph_rows_inv(m, pl[0], smem, s_red, t, a.h_rows, m.k14[ik ^ 1], &es, s_c4);
+                const double sum = ph_rows_inv<SX>(m, pl[0], smem, s_red, t, a.h_rows, m.k14[ik ^ 1], &es, s_c4);
                 if (tid == 0) m.partial[t] = sum;
                 t += G;
                 if (t < a.n_rows) {
@@ -228,7 +231,21 @@ size_t persist_layout(int nx, int ny, int Mx, int My, int K, int fwd_bytes, int 
     return ws + (size_t)ntw * sizeof(float2) + (K <= TICE_MAX ? (size_t)K * sizeof(double) : 0);
 }
 
-__global__ void __launch_bounds__(RT, 2) k_persist(PersistArgs a) { persist_body(a); }
-__global__ void __launch_bounds__(RT, 1) k_persist1(PersistArgs a) { persist_body(a); }
+template <int SX, int SY>
+__global__ void __launch_bounds__(RT, 2) k_persist(PersistArgs a) { persist_body<SX, SY>(a); }
+template <int SX, int SY>
+__global__ void __launch_bounds__(RT, 1) k_persist1(PersistArgs a) { persist_body<SX, SY>(a); }
+
+// The compiled (row, column) sequence pairs: the tuned schedules of the square grids of
+// the benchmark configurations (350 = 5*5*2*7, 1024 = 8*4*8*4) and the runtime passes.
+const void* persist_kernel(int seqx, int seqy, int minb) {
+#define FI_PERSIST_PAIR(X, Y)                                                              \
+    if (seqx == X && seqy == Y)                                                            \
+        return minb == 1 ? (const void*)k_persist1<X, Y> : (const void*)k_persist<X, Y>;
+    FI_PERSIST_PAIR(5527, 5527)
+    FI_PERSIST_PAIR(8484, 8484)
+#undef FI_PERSIST_PAIR
+    return minb == 1 ? (const void*)k_persist1<0, 0> : (const void*)k_persist<0, 0>;
+}
 
 }  // namespace fi

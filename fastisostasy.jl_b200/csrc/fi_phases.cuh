@@ -386,6 +386,7 @@ __device__ inline void fwd_prefetch(const Member& m, const FwdScalars& s, unsign
 // previous stage's spectrum after the column pass; its rows [loU, hiU) are inverted
 // here (halo recomputed), its own rows stored to kdst (k2 or k3) and used for the
 // stage vector.  The prefetched copies have landed and s is final.
+template <int SX = 0>
 __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const FwdViews& v, const FftPlan& plan,
                                    unsigned char* ws, const RowRanges& rr, int h, float2* Sout, int inv_prev,
                                    const float2* Sprev, float* kdst) {
@@ -418,7 +419,7 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
             }
         }
         __syncthreads();
-        const float2* res = fft_batch<true, float>(zb, zb + npi * nx, plan, npi, nx);
+        const float2* res = fft_run<true, float, SX>(zb, zb + npi * nx, plan, npi, nx);
         for (int rl = ty; rl < hi - lo; rl += TY) {
             const float2* rz = res + (rl >> 1) * nx;
             const int q = rl & 1;
@@ -580,7 +581,7 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
         }
     }
     __syncthreads();
-    float2* res = fft_batch<false, float>(zb, zb + np * nx, plan, np, nx);
+    float2* res = fft_run<false, float, SX>(zb, zb + np * nx, plan, np, nx);
     // split the pair spectra, store the half-spectrum rows
     for (int p = ty; p < np; p += TY) {
         const int ra = rr.y0 + 2 * p;
@@ -601,6 +602,7 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
 // ---------------------------------------------------------------------------
 // columns (in place on S); cpart_out: this task's 4 corner terms
 // ---------------------------------------------------------------------------
+template <int SY = 0>
 __device__ inline void ph_cols(const Member& m, const FftPlan& plan, const float2* twx, unsigned char* ws, int tile,
                                int B, float2* S, double* cpart_out) {
     const int ny = m.ny, tid = threadIdx.x, nth = blockDim.x;
@@ -617,7 +619,7 @@ __device__ inline void ph_cols(const Member& m, const FftPlan& plan, const float
     cpa_bytes(mu, m.mult + (size_t)kx0 * ny, nb * ny * 4);
     cpa_wait();
     __syncthreads();
-    float2* r = fft_batch<false, float>(b0, b1, plan, nb, ny);
+    float2* r = fft_run<false, float, SY>(b0, b1, plan, nb, ny);
     float2* o = (r == b0) ? b1 : b0;
     for (int i = tid; i < nb * ny; i += nth) {
         const float sc = mu[i];
@@ -625,7 +627,7 @@ __device__ inline void ph_cols(const Member& m, const FftPlan& plan, const float
         r[i] = make_float2(v.x * sc, v.y * sc);
     }
     __syncthreads();
-    float2* q = fft_batch<true, float>(r, o, plan, nb, ny);
+    float2* q = fft_run<true, float, SY>(r, o, plan, nb, ny);
     for (int i = tid; i < nb * ny; i += nth) {
         const int b = i / ny, y = i - b * ny;
         S[(size_t)y * m.sp + kx0 + b] = q[i];
@@ -668,6 +670,7 @@ __device__ inline void inv_prefetch(const Member& m, const float2* S, unsigned c
 // Inverse rows of S (prefetched) into dst; corners4 (shared): the field's corner
 // values.  Returns (in every thread) the block's sum of squared scaled errors when
 // e != null.
+template <int SX = 0>
 __device__ inline double ph_rows_inv(const Member& m, const FftPlan& plan, unsigned char* ws, double* red, int tile,
                                      int h, float* dst, const ErrTerms* e, const double* corners4) {
     InvLayout L;
@@ -690,7 +693,7 @@ __device__ inline double ph_rows_inv(const Member& m, const FftPlan& plan, unsig
         }
     }
     __syncthreads();
-    const float2* res = fft_batch<true, float>(zb, zb + np * nx, plan, np, nx);
+    const float2* res = fft_run<true, float, SX>(zb, zb + np * nx, plan, np, nx);
     const double cs = cmean(corners4, m.border_v);
     const int n = (y1 - y0) * nx;
     const float* k1 = (const float*)(ws + L.k1);

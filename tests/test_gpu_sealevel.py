@@ -43,10 +43,20 @@ def test_sealevel_rhs_parity(form, bsl):
     ref.init()
     sim.init_problem()
     u = _u0(sim)
+
+    def surfaces():
+        # the masks change only in a sparse update: keep the surfaces they were made from
+        return (ref.get_field(abi.FIELDS["z_ss"]) - ref.get_field(abi.FIELDS["z_b"]),
+                ref.get_field(abi.FIELDS["H_af"]).copy())
+
+    w_gate, haf_gate = surfaces()
     for t in (0.5, 12.5, 12.7, 31.0):
         ug, dg = u.copy(), np.zeros_like(u)
         F.update_diagnostics(dg, ug, sim, t)
+        ns0 = ref.stats()["nsparse"]
         ur, dr = ref.rhs(t, F_(u))
+        if ref.stats()["nsparse"] > ns0:
+            w_gate, haf_gate = surfaces()
         assert rel_l2(F_(dg), dr) < TOL[form], (t, rel_l2(F_(dg), dr))
         for name in ("dz_ss", "columnanom_seawater", "H_water"):
             # the water column and its anomaly are differences of O(km) surfaces
@@ -56,23 +66,24 @@ def test_sealevel_rhs_parity(form, bsl):
             assert e < TOL[form] * (1 if name == "dz_ss" and form == "fp64" else 10), (t, name, e)
         for name in ("maskgrounded", "maskocean"):
             a, b = F_(sim.get_field(name)), ref.get_field(abi.FIELDS[name])
-            # a mask is a sign test of a difference of surfaces: cells within rounding of
-            # the sea surface may flip (FP64: a few cells, ~1e-13 m from the threshold)
-            assert np.mean(a != b) <= (0.01 if form == "fp32" else 0.002), (t, name, int(np.sum(a != b)))
-            if form == "fp64" and np.any(a != b):
-                w = ref.get_field(abi.FIELDS["z_ss"]) - ref.get_field(abi.FIELDS["z_b"])
-                haf = ref.get_field(abi.FIELDS["H_af"])
-                wl = F_(sim.get_field("z_ss")) - F_(sim.get_field("z_b"))
-                hl = F_(sim.get_field("H_af"))
+            # a mask is a sign test of a difference of surfaces: in FP64 only cells within
+            # rounding of the threshold may flip
+            if form == "fp64":
+                # maskocean flips at w = z_ss - z_b = 0, maskgrounded where H_af leaves 0, both
+                # taken at the last sparse update; FP64 may differ only within rounding of them
                 bad = np.nonzero(a != b)[0]
-                edge = np.minimum(np.abs(w), np.abs(haf))[bad]
-                assert edge.max() < 1e-6, (t, name, bad.tolist(), w[bad].tolist(), wl[bad].tolist(),
-                                           haf[bad].tolist(), hl[bad].tolist(), a[bad].tolist(), b[bad].tolist())
+                edge = np.abs(w_gate[bad]) if name == "maskocean" else np.abs(haf_gate[bad])
+                assert bad.size == 0 or edge.max() < 1e-6, (t, name, bad.tolist(), edge.tolist())
+            else:
+                assert np.mean(a != b) <= 0.01, (t, name, int(np.sum(a != b)))
         sg, sr = sim.sealevel_state(), ref.sealevel()
         assert abs(sg["z_bsl"] - sr["z_bsl"]) <= 1e-9 * max(1.0, abs(sr["z_bsl"])), (t, sg, sr)
         if form == "fp64":
+            vol = abs(sr["V_af"]) + abs(sr["V_den"]) + abs(sr["V_pov"])
             for k in ("V_af", "V_den", "V_pov", "delta_V", "A_bsl"):
-                assert abs(sg[k] - sr[k]) <= 1e-9 * max(1.0, abs(sr[k])), (t, k, sg[k], sr[k])
+                # delta_V is a difference of volume sums (~1e15 m^3): rounding of the sums
+                scale = max(1.0, vol) if k == "delta_V" else max(1.0, abs(sr[k]))
+                assert abs(sg[k] - sr[k]) <= 1e-9 * scale, (t, k, sg[k], sr[k])
     assert np.abs(ref.get_field(abi.FIELDS["columnanom_seawater"])).max() > 0
     ref.close()
     sim.close()

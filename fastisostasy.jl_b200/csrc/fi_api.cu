@@ -244,6 +244,7 @@ static void copy_plan(const Plan& q, FftPlan& dst) {
     memcpy(dst.ns, q.ns, sizeof(dst.ns));
     dst.tw32 = q.tw32;
     dst.tw64 = q.tw64;
+    dst.seq = seq_code(q.radix, q.npass);
 }
 
 // The FP32 kernels read the plans from the member descriptor (staged in shared memory);
@@ -269,6 +270,7 @@ static int upload_plans(fi_handle* h) {
         memcpy(v[i].ns, h->plans[i].ns, sizeof(v[i].ns));
         v[i].tw32 = h->plans[i].tw32;
         v[i].tw64 = h->plans[i].tw64;
+        v[i].seq = seq_code(h->plans[i].radix, h->plans[i].npass);
     }
     if (!h->d_plans || h->n_plans_dev != v.size()) {
         RET(dalloc(h, &h->d_plans, v.size()));
@@ -2147,6 +2149,7 @@ struct fi_ensemble {
     unsigned long long* d_counter = nullptr;
     unsigned long long* d_trace = nullptr;
     EnsArgs args{};
+    const void* kfn = nullptr;  // the ensemble kernel build (ens_kernel)
     int grid = 0;
     size_t smem = 0;
     long long launches = 0;
@@ -2187,10 +2190,12 @@ static bool ensemble_setup_persist(fi_ensemble* e) {
     a = EnsArgs{};
     const size_t smem = ens_layout(hm.data(), n, &a);
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, k_ens) != cudaSuccess) return false;
+    const char* es = getenv("FI_ENS_SEQ");
+    e->kfn = ens_kernel(!(es && es[0] == '0'));
+    if (cudaFuncGetAttributes(&fa, e->kfn) != cudaSuccess) return false;
     if (smem + fa.sharedSizeBytes + 1024 > (size_t)smax) return false;
-    if (cudaFuncSetAttribute(k_ens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens, ROW_THREADS, smem) != cudaSuccess || occ < 1)
+    if (cudaFuncSetAttribute(e->kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, e->kfn, ROW_THREADS, smem) != cudaSuccess || occ < 1)
         return false;
     const bool okk = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
                      cudaEventCreate(&e->e0) == cudaSuccess && cudaEventCreate(&e->e1) == cudaSuccess &&
@@ -2333,7 +2338,7 @@ static int ensemble_step_persist(fi_ensemble* e, std::vector<std::vector<double>
             return FI_ERR_CUDA;
         void* args[] = {(void*)&e->args};
         cudaEventRecord(e->e0, e->stream);
-        cudaError_t ce = cudaLaunchCooperativeKernel((const void*)k_ens, dim3(e->grid), dim3(ROW_THREADS), args,
+        cudaError_t ce = cudaLaunchCooperativeKernel(e->kfn, dim3(e->grid), dim3(ROW_THREADS), args,
                                                      e->smem, e->stream);
         cudaEventRecord(e->e1, e->stream);
         unsigned int bar[4] = {0, 0, 0, 0};

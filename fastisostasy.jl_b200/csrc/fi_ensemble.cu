@@ -160,6 +160,7 @@ __device__ __forceinline__ int find_member(const EnsPlan& P, int n, int t) {
     return lo;
 }
 
+template <int ENS_SEQ>
 __global__ void __launch_bounds__(RT, 2) k_ens(EnsArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ EnsPlan P;
@@ -278,7 +279,7 @@ __global__ void __launch_bounds__(RT, 2) k_ens(EnsArgs a) {
                         __syncthreads();
                         if (inv && tile == 0 && tid == 0)
                             for (int q = 0; q < 4; q++) C.m.ctl->kcorner[stage == 3 ? 2 : 3][q] = C.c4[q];
-                        ph_rows_fwd(C.m, C.fs, C.fv, C.pl, ws, rr, C.m.h_rows, C.m.S[stage == 3 ? 1 : 0], inv,
+                        ph_rows_fwd<ENS_SEQ>(C.m, C.fs, C.fv, C.pl, ws, rr, C.m.h_rows, C.m.S[stage == 3 ? 1 : 0], inv,
                                     Sprev, stage == 3 ? C.m.k2 : C.m.k3);
                     }
                 base += phase_span(total, K, G);
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(RT, 2) k_ens(EnsArgs a) {
                         const int ai = find_member(P, P.nact, t);
                         const int m = P.act[ai], tile = t - P.off[ai];
                         if (C.cm != m) cache_member(a, C, m, 1, tw_smem, nullptr);
-                        ph_cols(C.m, C.pl, C.m.px.tw32, ws, tile, C.m.B_cols, C.m.S[stage == 3 ? 1 : 0],
+                        ph_cols<ENS_SEQ>(C.m, C.pl, C.m.px.tw32, ws, tile, C.m.B_cols, C.m.S[stage == 3 ? 1 : 0],
                                 C.m.cpart + 4 * tile);
                         if (tile == 0 && tid == 0) {
                             Ctl* gc = C.m.ctl;
@@ -348,7 +349,7 @@ __global__ void __launch_bounds__(RT, 2) k_ens(EnsArgs a) {
                     __syncthreads();
                     const int ik = C.c.ik;
                     const double sum =
-                        ph_rows_inv(C.m, C.pl, ws, s_red, tile, C.m.h_rows, C.m.k14[ik ^ 1], &C.es, C.c4);
+                        ph_rows_inv<ENS_SEQ>(C.m, C.pl, ws, s_red, tile, C.m.h_rows, C.m.k14[ik ^ 1], &C.es, C.c4);
                     if (tid == 0) {
                         C.m.partial[tile] = sum;
                         if (tile == 0)
@@ -394,6 +395,13 @@ size_t ens_layout(const Member* host_mems, int n, EnsArgs* a) {
     a->tw_cap = twc;
     a->tice_cap = tic;
     return (size_t)a->ws_bytes + (size_t)twc * sizeof(float2) + (size_t)tic * sizeof(double);
+}
+
+// The ensemble kernel whose row and column transforms dispatch per task on the
+// member's schedule (compiled sequences of the grids 64 .. 256), or with dispatch = 0
+// the one that runs every plan's runtime passes.
+const void* ens_kernel(int dispatch) {
+    return dispatch ? (const void*)k_ens<SEQ_DISPATCH> : (const void*)k_ens<0>;
 }
 
 }  // namespace fi

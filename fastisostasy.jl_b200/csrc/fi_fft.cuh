@@ -46,6 +46,8 @@ struct FftPlan {
     int ns[FFT_MAX_PASSES];
     const float2* tw32;
     const double2* tw64;
+    int seq;  // seq_code of the schedule (0: none), for kernels that dispatch on it
+    int pad_seq;
 };
 
 __host__ __device__ inline unsigned int fastdiv_magic(unsigned int d) {
@@ -342,13 +344,28 @@ __device__ __forceinline__ cplx<T>* fft_batch_ct(cplx<T>* src, cplx<T>* dst, con
     }
 }
 
-// the compiled sequence SEQ (the caller has matched it to the plan), or the runtime
-// passes of the plan when SEQ == 0
+// The sequences the ensemble kernel dispatches on per task (SEQ_DISPATCH): the tuned
+// schedules of its member grids 64, 96, 128, 192 and 256.
+constexpr int SEQ_DISPATCH = -1;
+
+// the compiled sequence SEQ (the caller has matched it to the plan), the runtime passes
+// of the plan when SEQ == 0, or (SEQ_DISPATCH) the compiled sequence of the plan's own
+// schedule when it is one of the ensemble set, else its runtime passes
 template <bool INV, typename T, int SEQ>
 __device__ __forceinline__ cplx<T>* fft_run(cplx<T>* buf0, cplx<T>* buf1, const FftPlan& p, int nbatch,
                                             int bstride) {
     if constexpr (SEQ == 0) {
         return fft_batch<INV, T>(buf0, buf1, p, nbatch, bstride);
+    } else if constexpr (SEQ == SEQ_DISPATCH) {
+        const cplx<T>* tw = plan_tw<T>(p);
+        switch (p.seq) {
+            case 444: return fft_batch_ct<INV, T, 444>(buf0, buf1, tw, nbatch, bstride);
+            case 834: return fft_batch_ct<INV, T, 834>(buf0, buf1, tw, nbatch, bstride);
+            case 484: return fft_batch_ct<INV, T, 484>(buf0, buf1, tw, nbatch, bstride);
+            case 838: return fft_batch_ct<INV, T, 838>(buf0, buf1, tw, nbatch, bstride);
+            case 2288: return fft_batch_ct<INV, T, 2288>(buf0, buf1, tw, nbatch, bstride);
+            default: return fft_batch<INV, T>(buf0, buf1, p, nbatch, bstride);
+        }
     } else {
         return fft_batch_ct<INV, T, SEQ>(buf0, buf1, plan_tw<T>(p), nbatch, bstride);
     }

@@ -75,7 +75,9 @@ struct EnsArgs {
     int tice_cap;                // doubles of the staged ice-time table
     unsigned long long* trace;   // optional phase timeline
 };
-__global__ void k_ens(EnsArgs a);
+// the ensemble kernel: dispatch 1 runs the compiled radix sequences of the member
+// grids where a member's schedule has one, 0 always the plans' runtime passes
+const void* ens_kernel(int dispatch);
 size_t ens_layout(const Member* host_mems, int n, EnsArgs* a);
 
 // ---- FP64 transforms and set-up (fi_setup.cu) ----

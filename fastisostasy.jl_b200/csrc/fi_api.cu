@@ -1672,12 +1672,14 @@ static int setup_persist(fi_handle* h, int K) {
         h->executor = EXEC_GRAPH;
         return FI_OK;
     }
-    // the 2-blocks-per-SM build where shared memory fits two blocks, else the one sized
-    // for a single block (more registers, no spills); FI_PERSIST_MINB=1|2 forces one
+    // the 2-blocks-per-SM build where shared memory fits two blocks and the row or
+    // column tasks outnumber the SMs, else the one sized for a single block (more
+    // registers, no spills: with at most one task per SM a second block only adds barrier
+    // arrivals); FI_PERSIST_MINB=1|2 forces one
     CK(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     CK(cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k2, ROW_THREADS, smem));
-    h->persist_minb = occ >= 2 ? 2 : 1;
+    h->persist_minb = (occ >= 2 && std::max(h->n_rows, h->n_cols) > nsm) ? 2 : 1;
     const char* mb = getenv("FI_PERSIST_MINB");
     if (mb && (mb[0] == '1' || mb[0] == '2')) h->persist_minb = mb[0] - '0';
     if (h->persist_minb == 1) {

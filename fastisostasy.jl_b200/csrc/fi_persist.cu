@@ -120,22 +120,21 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
             float2* Sout = m.S[stage == 3 ? 1 : 0];
             float* kdst = stage == 3 ? m.k2 : m.k3;
             int t = bid;
-            if (tid == 0) {
+            // warps 0-3 sum the previous stage's corner partials while a thread of warp 4
+            // sets up the stage's scalars; then the views and the corner offsets
+            if (inv) corners_from_partials_g(m.cpart, m.ncols, s_c4);
+            if (tid == 128) {
                 fwd_static(m, sc, stage, nullptr, tice, fs);
                 if (fs.status != FI_OK) sc.status = fs.status;
             }
             __syncthreads();
             if (t < a.n_rows) fwd_prefetch(m, fs, smem, row_ranges(t, a.h_rows, ny), inv, Sprev, &fv);
-            if (inv) cpa_bytes(smem + m.fl.cpart, m.cpart, m.ncols * 32);
-            cpa_wait();
-            __syncthreads();
-            if (inv) {
-                corners_from_partials((const double*)(smem + m.fl.cpart), m.ncols, s_c4);
-                __syncthreads();
-                if (tid == 0)
+            if (tid == 0) {
+                if (inv)
                     for (int q = 0; q < 4; q++) sc.kcorner[stage == 3 ? 2 : 3][q] = s_c4[q];
+                fwd_offsets(m, sc, s_uc, fs);
             }
-            if (tid == 0) fwd_offsets(m, sc, s_uc, fs);
+            cpa_wait();
             __syncthreads();
             while (t < a.n_rows) {
                 ph_rows_fwd<SX>(m, fs, fv, pl[0], smem, row_ranges(t, a.h_rows, ny), a.h_rows, Sout, inv, Sprev, kdst);
@@ -177,10 +176,8 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
             inv_layout(nx, a.h_rows, m.ncols, &L);
             int t = bid;
             if (t < a.n_rows) inv_prefetch(m, m.S[0], smem, t, a.h_rows, &es);
-            cpa_bytes(smem + L.cpart, m.cpart, m.ncols * 32);
+            corners_from_partials_g(m.cpart, m.ncols, s_c4);
             cpa_wait();
-            __syncthreads();
-            corners_from_partials((const double*)(smem + L.cpart), m.ncols, s_c4);
             __syncthreads();
             while (t < a.n_rows) {
                 const double sum = ph_rows_inv<SX>(m, pl[0], smem, s_red, t, a.h_rows, m.k14[ik ^ 1], &es, s_c4);

@@ -232,6 +232,18 @@ __device__ __forceinline__ void corners_from_partials(const double* cp, int ncol
     }
 }
 
+// the same sum read straight from the global partials (L2: other blocks wrote them
+// before the last grid barrier), in the same order, so the result is identical
+__device__ __forceinline__ void corners_from_partials_g(const double* cp, int ncols, double* out4) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w < 4) {
+        double acc = 0.0;
+        for (int t = lane; t < ncols; t += 32) acc += __ldcg(cp + 4 * t + w);
+        acc = warp_sum(acc);
+        if (lane == 0) out4[w] = acc;
+    }
+}
+
 // this column task's share of corner value qc (0: (0,0), 1: (nx-1,0), 2: (0,ny-1),
 // 3: (nx-1,ny-1)): terms kx0..kx0+nb-1 of the inverse real DFT of row 0 or ny-1
 // (q: the task's columns, y fastest)

@@ -30,7 +30,7 @@ namespace fi {
 // k_persist1 for one (no spills) where it fits only one.
 // SX / SY: the compiled radix sequences of the row and column transforms (0: the
 // plans' runtime passes).
-template <int SX, int SY>
+template <int SX, int SY, int WIDE>
 __device__ __forceinline__ void persist_body(const PersistArgs& a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ Member sm;
@@ -137,7 +137,7 @@ __device__ __forceinline__ void persist_body(const PersistArgs& a) {
             cpa_wait();
             __syncthreads();
             while (t < a.n_rows) {
-                ph_rows_fwd<SX>(m, fs, fv, pl[0], smem, row_ranges(t, a.h_rows, ny), a.h_rows, Sout, inv, Sprev, kdst);
+                ph_rows_fwd<SX, WIDE>(m, fs, fv, pl[0], smem, row_ranges(t, a.h_rows, ny), a.h_rows, Sout, inv, Sprev, kdst);
                 t += G;
                 if (t < a.n_rows) {
                     fwd_prefetch(m, fs, smem, row_ranges(t, a.h_rows, ny), inv, Sprev, &fv);
@@ -229,9 +229,9 @@ size_t persist_layout(int nx, int ny, int Mx, int My, int K, int fwd_bytes, int 
 }
 
 template <int SX, int SY>
-__global__ void __launch_bounds__(RT, 2) k_persist(PersistArgs a) { persist_body<SX, SY>(a); }
+__global__ void __launch_bounds__(RT, 2) k_persist(PersistArgs a) { persist_body<SX, SY, 0>(a); }
 template <int SX, int SY>
-__global__ void __launch_bounds__(RT, 1) k_persist1(PersistArgs a) { persist_body<SX, SY>(a); }
+__global__ void __launch_bounds__(RT, 1) k_persist1(PersistArgs a) { persist_body<SX, SY, 1>(a); }
 
 // The compiled (row, column) sequence pairs: the tuned schedules of the square grids of
 // the benchmark configurations (350 = 5*5*2*7, 1024 = 8*4*8*4) and the runtime passes.

@@ -398,7 +398,11 @@ __device__ inline void fwd_prefetch(const Member& m, const FwdScalars& s, unsign
 // previous stage's spectrum after the column pass; its rows [loU, hiU) are inverted
 // here (halo recomputed), its own rows stored to kdst (k2 or k3) and used for the
 // stage vector.  The prefetched copies have landed and s is final.
-template <int SX = 0>
+// WIDE (the one-block-per-SM build, whose register budget allows it): each thread issues
+// the loads of several of its elements before the first use, so a sub-step pays one
+// memory round trip per group instead of one per element; the elements and their
+// arithmetic are the same, so the results are identical.
+template <int SX = 0, int WIDE = 0>
 __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const FwdViews& v, const FftPlan& plan,
                                    unsigned char* ws, const RowRanges& rr, int h, float2* Sout, int inv_prev,
                                    const float2* Sprev, float* kdst) {
@@ -454,12 +458,32 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
         const double a1 = s.a1, a2 = s.a2, a3 = s.a3, c1 = s.c1, c2 = s.c2, c3 = s.c3, off = s.off;
         const int nU = (rr.hiU - rr.loU) * nx;
         const double* ub = L.stage_u ? sU : s.uprev + (size_t)rr.loU * nx;
-        for (int i = tid; i < nU; i += RT) {
-            double u = ub[i];
-            if (a1 != 0.0) u += a1 * ((double)k1[i] - c1);
-            if (a2 != 0.0) u += a2 * ((double)k2[i] - c2);
-            if (a3 != 0.0) u += a3 * ((double)k3[i] - c3);
-            sU[i] = u - off;
+        // ub may alias sU: every element is read before it is written
+        constexpr int BQ = WIDE ? 4 : 1;
+        for (int i0 = tid; i0 < nU; i0 += BQ * RT) {
+            double ur[BQ];
+            float q1[BQ], q2[BQ], q3[BQ];
+#pragma unroll
+            for (int q = 0; q < BQ; q++) {
+                const int i = i0 + q * RT;
+                if (i < nU) {
+                    ur[q] = ub[i];
+                    q1[q] = a1 != 0.0 ? k1[i] : 0.0f;
+                    q2[q] = a2 != 0.0 ? k2[i] : 0.0f;
+                    q3[q] = a3 != 0.0 ? k3[i] : 0.0f;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < BQ; q++) {
+                const int i = i0 + q * RT;
+                if (i < nU) {
+                    double u = ur[q];
+                    if (a1 != 0.0) u += a1 * ((double)q1[q] - c1);
+                    if (a2 != 0.0) u += a2 * ((double)q2[q] - c2);
+                    if (a3 != 0.0) u += a3 * ((double)q3[q] - c3);
+                    sU[i] = u - off;
+                }
+            }
         }
     }
     __syncthreads();
@@ -480,7 +504,16 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
             else { Ua = Ur + nx; Ub = Ur - nx; sy = i2dy; }
             const int mo = (r - rr.loM) * nx;
             const float* Dr = v.D + (r - rr.loM) * nx;
-            for (int x = tx; x < nx; x += TX) {
+            constexpr int BX = WIDE ? 3 : 1;
+            for (int x0 = tx; x0 < nx; x0 += BX * TX) {
+            float Dq[BX];
+#pragma unroll
+            for (int q = 0; q < BX; q++)
+                if (x0 + q * TX < nx) Dq[q] = Dr[x0 + q * TX];
+#pragma unroll
+            for (int q = 0; q < BX; q++) {
+                const int x = x0 + q * TX;
+                if (x >= nx) continue;
                 const int xc = min(max(x, 1), nx - 2);
                 const double uxx = (Ur[xc + 1] - 2.0 * Ur[xc] + Ur[xc - 1]) * idx2;
                 const double uyy = (U0[nx + x] - 2.0 * U0[x] + U0[x - nx]) * idy2;
@@ -489,10 +522,11 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
                 else if (x == nx - 1) { da = (Ua[nx - 1] - Ua[nx - 2]) * idx; db = (Ub[nx - 1] - Ub[nx - 2]) * idx; }
                 else { da = (Ua[x + 1] - Ua[x - 1]) * i2dx; db = (Ub[x + 1] - Ub[x - 1]) * i2dx; }
                 const double uxy = (da - db) * sy;
-                const double D = (double)Dr[x];
+                const double D = (double)Dq[q];
                 sMxx[mo + x] = (float)(-D * (nu * uyy + uxx));
                 sMyy[mo + x] = (float)(-D * (nu * uxx + uyy));
                 sMxy[mo + x] = (float)(-D * (1.0 - nu) * uxy);
+            }
             }
         }
     }
@@ -504,15 +538,32 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
         const int flags = m.flags;
         const int n_own = (rr.y1 - rr.y0) * nx;
         const double* Uown = sU + (rr.y0 - rr.loU) * nx;
-        for (int i = tid; i < n_own; i += RT) {
+        constexpr int BI = WIDE ? 3 : 1;
+        for (int i0 = tid; i0 < n_own; i0 += BI * RT) {
+        float qa[BI], qb[BI], qe[BI], qz[BI], qd[BI];
+#pragma unroll
+        for (int q = 0; q < BI; q++) {
+            const int i = i0 + q * RT;
+            if (i < n_own) {
+                qa[q] = v.Ha[i];
+                qb[q] = fw != 0.0f ? v.Hb[i] : 0.0f;
+                qe[q] = v.ue[i];
+                qz[q] = v.uz[i];
+                qd[q] = v.dz[i];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < BI; q++) {
+            const int i = i0 + q * RT;
+            if (i >= n_own) continue;
             const int g = rr.y0 * nx + i;
             const double u = Uown[i];
-            const float ha = v.Ha[i];
-            const double H = (double)(fw != 0.0f ? ha + (v.Hb[i] - ha) * fw : ha);
-            const double uev = (double)v.ue[i] - cue;
-            const double dzv = (double)v.dz[i] - cdz;
+            const float ha = qa[q];
+            const double H = (double)(fw != 0.0f ? ha + (qb[q] - ha) * fw : ha);
+            const double uev = (double)qe[q] - cue;
+            const double dzv = (double)qd[q] - cdz;
             const double zdiff = (double)((flags & FLAG_ZBSS) ? v.zbss[i] : m.zbss_scalar) +
-                                 ((double)v.uz[i] - cuz) + u - dzv - s.dzbsl;
+                                 ((double)qz[q] - cuz) + u - dzv - s.dzbsl;
             double haf = H + (zdiff < 0.0 ? zdiff : 0.0) * m.rho_sw_ice;
             haf = haf > 0.0 ? haf : 0.0;
             const double mk = (flags & FLAG_MASK) ? (double)v.mask[i] : 1.0;
@@ -548,6 +599,7 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
             sR[i] = (float)(-m.g * sfull);
             if (unew) unew[g] = u;
         }
+        }
     }
     __syncthreads();
     // 3: moment divergence in FP32 -> f = rhs * K/(2 eta), rows packed in pairs
@@ -574,7 +626,16 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
             float* zrow = (float*)(zb + p * nx) + q;
             const float* vf = v.visc + (rv - rr.y0) * nx;
             const float* sr = sR + (rv - rr.y0) * nx;
-            for (int x = tx; x < nx; x += TX) {
+            constexpr int BV = WIDE ? 3 : 1;
+            for (int x0 = tx; x0 < nx; x0 += BV * TX) {
+            float vq[BV];
+#pragma unroll
+            for (int k = 0; k < BV; k++)
+                vq[k] = (valid && x0 + k * TX < nx) ? vf[x0 + k * TX] : 0.0f;
+#pragma unroll
+            for (int k = 0; k < BV; k++) {
+                const int x = x0 + k * TX;
+                if (x >= nx) continue;
                 float f = 0.0f;
                 if (valid) {
                     const int xc = min(max(x, 1), nx - 2);
@@ -586,9 +647,10 @@ __device__ inline void ph_rows_fwd(const Member& m, const FwdScalars& s, const F
                     else { da = (Ma[x + 1] - Ma[x - 1]) * i2dx; db = (Mb[x + 1] - Mb[x - 1]) * i2dx; }
                     const float mxy = (da - db) * sy;
                     const float rhs = sr[x] + (mxx + (2.0f * mxy + myy));
-                    f = rhs * vf[x];
+                    f = rhs * vq[k];
                 }
                 zrow[2 * x] = f;
+            }
             }
         }
     }

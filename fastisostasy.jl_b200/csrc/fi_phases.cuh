@@ -191,6 +191,11 @@ __device__ __forceinline__ void cpa_bytes(void* dst, const void* src, int bytes)
     }
 }
 
+// the same, called out of line: the optional input staging of the forward row phase,
+// kept out of the phase's instruction stream (with inputs read in place it never runs,
+// and its inlined copy loops would only spread the executed code over more cache lines)
+static __device__ __noinline__ void cpa_bytes_ool(void* dst, const void* src, int bytes) { cpa_bytes(dst, src, bytes); }
+
 // cooperative copy of a struct (8-byte words) by all threads of the block
 __device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes) {
     const unsigned long long* s = (const unsigned long long*)src;
@@ -205,7 +210,7 @@ __device__ __forceinline__ const T* stage_rows(unsigned char* ws, int off, const
     const T* src = g + (size_t)r0 * nx;
     if (off < 0 || !g) return src;
     T* dst = (T*)(ws + off);
-    cpa_bytes(dst, src, (r1 - r0) * nx * (int)sizeof(T));
+    cpa_bytes_ool(dst, src, (r1 - r0) * nx * (int)sizeof(T));
     return dst;
 }
 
@@ -352,11 +357,11 @@ __device__ inline void fwd_prefetch(const Member& m, const FwdScalars& s, unsign
     const FwdLayout& L = m.fl;
     const int nx = m.nx, stage = s.stage;
     const bool t0 = threadIdx.x == 0;
-    if (L.stage_u) cpa_bytes(ws + L.U, s.uprev + (size_t)rr.loU * nx, (rr.hiU - rr.loU) * nx * 8);
+    if (L.stage_u) cpa_bytes_ool(ws + L.U, s.uprev + (size_t)rr.loU * nx, (rr.hiU - rr.loU) * nx * 8);
     if (inv_prev && L.S_in >= 0) {
         // spectrum rows have pitch sp; copy the NH used entries of each row
         for (int r = rr.loU; r < rr.hiU; r++)
-            cpa_bytes(ws + L.S_in + (size_t)(r - rr.loU) * m.NH * 8, Sprev + (size_t)r * m.sp, m.NH * 8);
+            cpa_bytes_ool(ws + L.S_in + (size_t)(r - rr.loU) * m.NH * 8, Sprev + (size_t)r * m.sp, m.NH * 8);
         if (t0) vsh->S = (const float2*)(ws + L.S_in);
     } else if (t0) {
         vsh->S = nullptr;

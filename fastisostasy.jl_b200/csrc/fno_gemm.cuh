@@ -244,14 +244,20 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(TcGemmArgs g, Epi epi) {
     tc_fence_after();
     const uint32_t tmem = tmem_base;
     const uint32_t idesc = tc_instr_desc(TC_BM, BN);
-    // output tile and chunk of job j
+    // output tile and chunk of job j, in 32-bit arithmetic (the launch checks that tiles x
+    // chunks fit; 64-bit divisions cost ~10x more instructions in every thread)
+    const unsigned umnt = (unsigned)mt * (unsigned)nt, unch = (unsigned)nch, umt = (unsigned)mt;
     auto job = [&](long long j, int& m0, int& n0, int& z, int& c) {
-        const long long tile = blockIdx.x + (j / nch) * gridDim.x;
-        c = (int)(j % nch);
-        const long long mn = tile % ((long long)mt * nt);
-        z = (int)(tile / ((long long)mt * nt));
-        m0 = (int)(mn % mt) * TC_BM;
-        n0 = (int)(mn / mt) * BN;
+        const unsigned jj = (unsigned)j;
+        const unsigned jq = jj / unch;
+        const unsigned tile = blockIdx.x + jq * gridDim.x;
+        c = (int)(jj - jq * unch);
+        const unsigned zt = tile / umnt;
+        const unsigned mn = tile - zt * umnt;
+        z = (int)zt;
+        const unsigned nq = mn / umt;
+        m0 = (int)(mn - nq * umt) * TC_BM;
+        n0 = (int)nq * BN;
     };
     auto stage = [&](long long j) {
         int m0, n0, z, c;
@@ -369,7 +375,8 @@ inline cudaError_t launch_gemm_tc(const TcGemmArgs& g, int batch, const Epi& epi
     const long long ntiles =
         (long long)((g.M + TC_BM - 1) / TC_BM) * ((g.N + BN - 1) / BN) * (long long)batch;
     if (ntiles <= 0) return cudaSuccess;
-    if (ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+    if (ntiles > 0x7fffffffLL || ntiles * (long long)((g.K + TC_BK - 1) / TC_BK) > 0x7fffffffLL)
+        return cudaErrorInvalidValue;
     k_gemm_tc<BN, Epi><<<(unsigned)ntiles, TC_THREADS, 2 * STAGE, st>>>(a, epi);
     return cudaGetLastError();
 }

@@ -22,11 +22,11 @@
 //   ph_conv_*       padded linear convolutions of the elastic and sea-surface loads
 //                   (convolutions.jl:94-154), crop window + raw corner values.
 //
-// Latency: every row and column phase first issues all of its global inputs as
-// asynchronous copies into shared memory (cp.async), waits once, and then computes
-// from shared memory, so a phase costs one memory round trip instead of one per
-// dependent load.  Inputs that do not fit the member's shared-memory budget are read
-// in place from global memory by the same code (FwdLayout offset -1).
+// Latency: the column and inverse-row phases first issue their global inputs as
+// asynchronous copies into shared memory (cp.async), wait once, and then compute from
+// shared memory.  The forward-row phase reads its inputs in place by default (measured
+// faster: its sub-steps hide the loads), or stages them the same way where the member's
+// shared-memory budget allows and staging is selected (FwdLayout offset -1: in place).
 //
 // The corner values of a dudt field (the dudt corner BC, deformation.jl:101) come from
 // the column pass: each column task adds its columns' terms of the inverse real DFT
